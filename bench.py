@@ -1,0 +1,430 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the B200 D3Q19 TRT kernels.
+
+Workload (N=1, per rank for N>1): a 256^3 fully periodic box filled with a
+seeded packing of solid spheres (radius uniform in [6, 12], porosity 0.40,
+about 6.7M fluid nodes), FP64 PDFs, TRT with Lambda = 3/16, omega = 1, body
+force along x. The headline kernel is the list AA kernel
+("cuda-list-aa-pv-soa", the drop-in for the reference's list-aa-pv-soa). A
+"step" is one time step over all fluid nodes.
+
+  value     MFLUP/s over exactly K device-timed steps (CUDA events on the
+            kernel stream), inputs resident in HBM (1.3 GB of PDFs, larger than
+            the 126 MB L2), max over ranks
+  e2e       the same metric through the reference-facing C ABI: one Kernel()
+            call of the configuration's 500 steps with the PDF field uploaded
+            from the pinned host mirror before and downloaded after
+  roofline  the dominant kernel (the odd, adjacency-driven step): algorithmic
+            bytes per launch / mean launch time, against the measured HBM copy
+            bandwidth in MEASURED_PEAKS.json
+  cpu_baseline  the reference's own list-aa-pv-soa (compiled from its sources
+            into oracle/_ref) on this host's cores, a bounded sample of the
+            same domain
+
+`--impl reference` times the reference's CPU kernel alone on the same
+workload and prints its own line. For N>1 every rank runs its own domain (seed
++ rank): no data moves between ranks, scaling is weak.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "lbm-benchmark-kernels_b200")
+sys.path.insert(0, PKG)
+
+L2_BYTES = 126 * 1024 * 1024
+B_PER_FLUP = {"even": 2 * 19 * 8, "odd": 2 * 19 * 8 + 18 * 4, "pull": 2 * 19 * 8 + 18 * 4, "aa": 2 * 19 * 8}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=500)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--edge", type=int, default=256)
+    p.add_argument("--porosity", type=float, default=0.40)
+    p.add_argument("--seed", type=int, default=20251203)
+    p.add_argument("--no-extra", action="store_true", help="skip the secondary kernel lines")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# ranks
+
+class Dist:
+    def __init__(self, n_gpus):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", self.local))
+            self.torch, self.dist = torch, dist
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, v):
+        if self.world == 1:
+            return v
+        t = self.torch.tensor([float(v)], device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v):
+        if self.world == 1:
+            return v
+        t = self.torch.tensor([float(v)], dtype=self.torch.float64, device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            m = json.load(f)
+        return float(m["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel_key):
+    """DRAM bytes per launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        t = json.load(f)
+    rec = t.get(kernel_key)
+    return None if rec is None else rec.get("bytes_per_launch_full")
+
+
+def sphere_lattice(lbmb200, edge, porosity, seed):
+    L = lbmb200.lib()
+    L.lbm_geo_spheres.argtypes = [ctypes.c_int * 3, ctypes.c_uint64, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_int, ctypes.POINTER(lbmb200.LatticeDesc),
+                                  ctypes.POINTER(ctypes.c_double)]
+    ld = lbmb200.LatticeDesc()
+    st = (ctypes.c_double * 4)()
+    dims = (edge, edge, edge)
+    rc = L.lbm_geo_spheres((ctypes.c_int * 3)(*dims), seed, porosity, 6.0, 12.0, 20000, ctypes.byref(ld), st)
+    if rc:
+        raise RuntimeError("sphere packing failed")
+    import numpy as np
+    n = edge ** 3
+    mask = np.ctypeslib.as_array(ld.Lattice, shape=(n,)).copy()
+    ctypes.CDLL(None).free(ctypes.cast(ld.Lattice, ctypes.c_void_p))
+    lat = lbmb200.Lattice(mask, dims, (1, 1, 1), "spheres")
+    stats = {"porosity": round(st[0], 6), "spheres_rsa": int(st[1]), "spheres_overlap": int(st[2]),
+             "jam_porosity": round(st[3], 4)}
+    return lat, stats
+
+
+def equilibrium_field(lbmb200, lat):
+    import numpy as np
+    return np.broadcast_to(lbmb200.W, (lat.mask.size, 19))
+
+
+def time_kernel(lbmb200, kname, lat, steps, warmup, kargs, dist, odd_key):
+    """Device-timed steps of one kernel instance; returns timing dict."""
+    import numpy as np
+    inst = lbmb200.kernel(kname).init(lat, kernel_args=kargs)
+    try:
+        inst.set_field(np.ascontiguousarray(equilibrium_field(lbmb200, lat)))
+        cd = lbmb200.case(omega=1.0, xforce=1e-5, iterations=steps)
+        L = lbmb200.lib()
+        tot = ctypes.c_double(0.0)
+        if warmup > 0:
+            rc = L.lbm_b200_time_steps(inst.kdp, ctypes.byref(cd), warmup, ctypes.byref(tot), None)
+            if rc:
+                raise RuntimeError(L.lbm_b200_last_error().decode())
+        n_launch = steps if "pull" in kname else 2 * ((steps + 1) // 2)
+        per = (ctypes.c_double * n_launch)()
+        dist.barrier()
+        rc = L.lbm_b200_time_steps(inst.kdp, ctypes.byref(cd), steps, ctypes.byref(tot), per)
+        if rc:
+            raise RuntimeError(L.lbm_b200_last_error().decode())
+        dist.barrier()
+        per = list(per)
+        res = {"ms": tot.value, "launches": n_launch, "steps_run": n_launch if "pull" in kname else n_launch,
+               "per_launch_ms": per, "inst": inst}
+        return res
+    except Exception:
+        inst.deinit()
+        raise
+
+
+class _StdoutToStderr:
+    """Sends C-level stdout to stderr (the reference prints its progress there),
+    so that stdout carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+
+    def __exit__(self, *exc):
+        ctypes.CDLL(None).fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def cpu_reference(lat, iterations, threads=None, variant=None):
+    """The reference's list-aa-pv-soa (benchmark build) on this host's cores."""
+    with _StdoutToStderr():
+        return _cpu_reference(lat, iterations, threads, variant)
+
+
+def _cpu_reference(lat, iterations, threads=None, variant=None):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Reference, reference_available
+    if variant is None:
+        flags = open("/proc/cpuinfo").read()
+        variant = "bench-avx512" if " avx512f" in flags and reference_available("bench-avx512") else "bench-avx2"
+    if not reference_available(variant):
+        return None
+    ref = Reference(variant)
+    threads = ref.set_threads(threads or os.cpu_count() or 1)
+    ref.run("list-aa-pv-soa", lat.dims, lat.periodic, lat.mask, omega=1.0, xforce=1e-5,
+            iterations=iterations, init="zero", want_pdfs=False)
+    dur = ref.last_duration
+    it = iterations + (iterations % 2)  # the AA loop runs whole pairs
+    return {"mflups": lat.n_fluid * it / dur / 1e6, "seconds": dur, "iterations": it, "threads": threads,
+            "variant": variant}
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ---------------------------------------------------------------------------
+
+def run_reference_arm(args, dist):
+    metric = "MFLUP/s & % HBM roofline at 256^3"
+    if dist.rank != 0:
+        return 0
+    import lbmb200
+    lat, stats = sphere_lattice(lbmb200, args.edge, args.porosity, args.seed)
+    if args.warmup > 0:
+        cpu_reference(lat, max(2, args.warmup))
+    r = cpu_reference(lat, args.steps)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref is missing"}))
+        return 0
+    line = {"impl": "reference", "metric": metric, "value": round(r["mflups"], 3), "unit": "MFLUP/s",
+            "n_gpus": args.gpus, "steps": r["iterations"], "warmup": args.warmup,
+            "ms_per_step": round(1e3 * r["seconds"] / r["iterations"], 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "%d^3 periodic sphere packing, porosity %.2f (%d fluid nodes), reference "
+                                   "list-aa-pv-soa, FP64" % (args.edge, stats["porosity"], lat.n_fluid),
+                       "kernel": "list-aa-pv-soa (reference, %s)" % r["variant"]},
+            "cpu_baseline": {"value": round(r["mflups"], 3), "unit": "MFLUP/s", "cores": r["threads"],
+                             "kind": "reference", "sample": "%d steps of the full domain" % r["iterations"],
+                             "cpu": cpu_model()},
+            "e2e": {"value": round(r["mflups"], 3), "unit": "MFLUP/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args, dist):
+    import numpy as np
+
+    import lbmb200
+    L = lbmb200.lib()
+    if L.lbm_b200_set_device(dist.local) != 0:
+        raise RuntimeError("cannot select CUDA device %d: %s" % (dist.local, L.lbm_b200_last_error().decode()))
+    peak, peak_kind = measured_peaks()
+    lat, stats = sphere_lattice(lbmb200, args.edge, args.porosity, args.seed + dist.rank)
+    kargs = ["-lambda", "3/16"]
+
+    clocks = ClockSampler(dist.local)
+    clocks.start()
+    t = time_kernel(lbmb200, "cuda-list-aa-pv-soa", lat, args.steps, max(3, args.warmup), kargs, dist, "odd")
+    inst = t["inst"]
+    try:
+        # e2e: the reference-facing Kernel() call, mirror uploaded and downloaded
+        cd = lbmb200.case(omega=1.0, xforce=1e-5, iterations=500)
+        L.lbm_b200_mark_mirror_dirty(inst.kdp)
+        dist.barrier()
+        w0 = time.perf_counter()
+        inst.run(cd)
+        e2e_s = time.perf_counter() - w0
+        e2e_s = dist.max(e2e_s)
+        h2d, d2h = inst.last_copy_bytes()
+        e2e_iters = 500
+        n_cells = inst.list_layout()[3]
+    finally:
+        inst.deinit()
+    clk = clocks.stop()
+
+    nf_total = dist.sum(lat.n_fluid)
+    ms = dist.max(t["ms"])
+    steps_run = t["launches"]
+    value = nf_total * steps_run / (ms / 1e3) / 1e6
+    per = t["per_launch_ms"]
+    even = per[0::2]
+    odd = per[1::2]
+    odd_ms = statistics.mean(odd)
+    even_ms = statistics.mean(even)
+    achieved = B_PER_FLUP["odd"] * lat.n_fluid / (odd_ms / 1e3) / 1e9
+    traffic = profile_traffic("list_odd_fp64")
+    line = {
+        "metric": "MFLUP/s & % HBM roofline at 256^3", "value": round(value, 3), "unit": "MFLUP/s",
+        "n_gpus": dist.world, "steps": steps_run, "warmup": max(3, args.warmup),
+        "ms_per_step": round(ms / steps_run, 5), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "%d^3 periodic sphere packing, porosity %.4f, r~U[6,12], seed %d+rank; "
+                               "cuda-list-aa-pv-soa, FP64, Lambda=3/16, omega=1, F_x=1e-5"
+                               % (args.edge, stats["porosity"], args.seed),
+                   "fluid_nodes_per_rank": lat.n_fluid, "packing": stats,
+                   "l2": "inputs larger than L2 (%.2f GB of PDFs per rank)" % (19 * 8 * n_cells / 1e9),
+                   "parallelism": "replicas" if dist.world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "kernel": "k_list_odd_fp64 (adjacency-driven odd step)",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "bytes_per_flup": B_PER_FLUP["odd"], "launch_ms": round(odd_ms, 5),
+                     "traffic": traffic,
+                     "even_step": {"bytes_per_flup": B_PER_FLUP["even"], "launch_ms": round(even_ms, 5),
+                                   "achieved": round(B_PER_FLUP["even"] * lat.n_fluid / (even_ms / 1e3) / 1e9, 1)}},
+        "e2e": {"value": round(nf_total * e2e_iters / e2e_s / 1e6, 3), "unit": "MFLUP/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "step": "one Kernel() call of 500 time steps with PDF upload and download"},
+        "gpu_launches": steps_run,
+        "clocks": clk,
+    }
+
+    if not args.no_extra:
+        extra = {}
+        # pull kernel on the same domain
+        tp = time_kernel(lbmb200, "cuda-list-pull-split-nt-1s-soa", lat, min(args.steps, 200), 3, kargs, dist, "pull")
+        tp["inst"].deinit()
+        pm = statistics.mean(tp["per_launch_ms"])
+        extra["cuda-list-pull-split-nt-1s-soa"] = {
+            "mflups": round(lat.n_fluid / (pm / 1e3) / 1e6, 1), "launch_ms": round(pm, 5),
+            "achieved_gbs": round(B_PER_FLUP["pull"] * lat.n_fluid / (pm / 1e3) / 1e9, 1),
+            "frac": round(B_PER_FLUP["pull"] * lat.n_fluid / (pm / 1e3) / 1e9 / peak, 4)}
+        # full-array AA on a fully periodic 256^3 box (the reference's -geometry fluid with
+        # -periodic-x -periodic-y -periodic-z)
+        fl = lbmb200.geometry("fluid", (args.edge,) * 3, (1, 1, 1))
+        ta = time_kernel(lbmb200, "cuda-aa-soa", fl, min(args.steps, 200), 4, kargs, dist, "aa")
+        ta["inst"].deinit()
+        am = statistics.mean(ta["per_launch_ms"])
+        ev = statistics.mean(ta["per_launch_ms"][0::2])
+        od = statistics.mean(ta["per_launch_ms"][1::2])
+        extra["cuda-aa-soa"] = {
+            "workload": "%d^3 fully periodic fluid box" % args.edge, "fluid_nodes": fl.n_fluid,
+            "mflups": round(fl.n_fluid / (am / 1e3) / 1e6, 1),
+            "achieved_gbs": round(B_PER_FLUP["aa"] * fl.n_fluid / (am / 1e3) / 1e9, 1),
+            "frac": round(B_PER_FLUP["aa"] * fl.n_fluid / (am / 1e3) / 1e9 / peak, 4),
+            "even_ms": round(ev, 5), "odd_ms": round(od, 5)}
+        line["kernels"] = extra
+
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
+        probe = cpu_reference(lat, 2)
+        if probe is not None:
+            # size the sample to about 10 s of CPU work
+            iters = int(max(4, min(400, 10.0 * probe["mflups"] * 1e6 / lat.n_fluid)))
+            r = cpu_reference(lat, iters)
+            line["cpu_baseline"] = {"value": round(r["mflups"], 3), "unit": "MFLUP/s", "cores": r["threads"],
+                                    "kind": "reference",
+                                    "sample": "%d steps of the same domain, reference list-aa-pv-soa (%s build), %s"
+                                              % (r["iterations"], r["variant"], cpu_model())}
+    if dist.rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    dist = Dist(args.gpus)
+    try:
+        if args.impl == "reference":
+            return run_reference_arm(args, dist)
+        return run_ours(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

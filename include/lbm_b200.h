@@ -1,0 +1,236 @@
+/* lbm_b200.h -- C ABI of the B200 (sm_100a) D3Q19 TRT kernels.
+ *
+ * The drop-in boundary is the reference benchmark's own kernel-table API:
+ *
+ *   typedef struct KernelFunctions_ { char Name[128];
+ *       void (*Init)(LatticeDesc *, KernelData **, Parameters *);
+ *       void (*Deinit)(LatticeDesc *, KernelData **); } KernelFunctions;
+ *                                                   (src/KernelFunctions.h:49-54)
+ *
+ * Each CUDA kernel below is one Init/Deinit pair with exactly those
+ * signatures. Init builds the device layout from the LatticeDesc mask, uploads
+ * it, and installs in the returned KernelData (src/Kernel.h:187-211):
+ *   Kernel   runs cd->MaxIterations time steps on the GPU (the AA kernels, as
+ *            in the reference, advance in even/odd pairs), synchronises, sets
+ *            Duration, and leaves a host mirror valid for GetNode;
+ *   GetNode / SetNode, BoundaryConditionsGetPdf / SetPdf
+ *            read and write the logical PDFs of a node through the mirror
+ *            (SetNode marks it for upload before the next Kernel call);
+ *   LoopBalance  the kernel's algorithmic bytes per fluid-lattice update.
+ * Errors print a message and exit(1), as the reference does.
+ *
+ * The structs are layout-compatible with the reference's (PdfT = double). If
+ * the reference's Kernel.h has been included first, its definitions are used.
+ *
+ * Library: liblbmb200.so (lbm-benchmark-kernels_b200/), built for sm_100a.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#ifndef __KERNEL_H__
+/* ---- reference-compatible types (src/Lattice.h:33-55, src/Kernel.h:172-222) ---- */
+typedef double PdfT;
+typedef int LatticeT;
+
+enum { LAT_CELL_OBSTACLE = 0, LAT_CELL_FLUID = 1, LAT_CELL_INLET = 2, LAT_CELL_OUTLET = 4 };
+
+typedef struct LatticeDesc_ {
+	int Dims[3];
+	LatticeT *Lattice;
+	int nCells;
+	int nFluid;
+	int nObst;
+	int nInlet;
+	int nOutlet;
+	int PeriodicX;
+	int PeriodicY;
+	int PeriodicZ;
+	const char *Name;
+} LatticeDesc;
+
+typedef struct CaseData_ {
+	PdfT Omega;
+	PdfT RhoIn;
+	PdfT RhoOut;
+	PdfT Ux;
+	PdfT Uy;
+	PdfT Uz;
+	PdfT XForce;
+	int MaxIterations;
+	int VtkOutput;
+	int VtkModulus;
+	int StatisticsModulus;
+} CaseData;
+
+typedef struct KernelData_ {
+	PdfT *Pdfs[2];
+	PdfT *SrcPdfs;
+	PdfT *DstPdfs;
+	PdfT *PdfsActive;
+	int Dims[3];
+	int GlobalDims[3];
+	int Offsets[3];
+	int *ObstIndices;
+	int nObstIndices;
+	int *BounceBackPdfsSrc;
+	int *BounceBackPdfsDst;
+	int nBounceBackPdfs;
+	double LoopBalance;
+	double Duration;
+	void (*BoundaryConditionsGetPdf)(struct KernelData_ *kd, int x, int y, int z, int dir, PdfT *pdf);
+	void (*BoundaryConditionsSetPdf)(struct KernelData_ *kd, int x, int y, int z, int dir, PdfT pdf);
+	void (*GetNode)(struct KernelData_ *kd, int x, int y, int z, PdfT *pdfs);
+	void (*SetNode)(struct KernelData_ *kd, int x, int y, int z, PdfT *pdfs);
+	void (*Kernel)(LatticeDesc *ld, struct KernelData_ *kd, CaseData *cd);
+} KernelData;
+
+typedef struct Parameters_ {
+	int nArgs;
+	char **Args;
+	int nKernelArgs;
+	char **KernelArgs;
+} Parameters;
+#endif /* __KERNEL_H__ */
+
+/* ---- kernel-table rows (drop-ins for src/KernelFunctions.h:56-188) ----
+ * Kernel arguments (after "--" on the command line, Parameters.KernelArgs):
+ *   -lambda <v|a/b>   TRT magic parameter (default 1/12, the value the
+ *                     reference hard-codes, e.g. src/BenchKernelD3Q19Aa.c:71)
+ *   -blk <n>, -blk-x/-blk-y/-blk-z <n>
+ *                     list kernels: blocked numbering of the fluid nodes, as
+ *                     src/BenchKernelD3Q19ListAaPvCommon.c:631-656
+ *   -pad auto|no|m+o[,m+o]*  list kernels: SoA padding (src/Padding.c:19-193)
+ *   -bs <n>           threads per block of the list kernels (default 256)
+ */
+
+/* "cuda-aa-soa": AA pattern, full array, SoA. Replaces D3Q19AaInit_AaSoA /
+ * D3Q19AaDeinit_AaSoA (src/BenchKernelD3Q19Aa.h:33-37, registered as "aa-soa"
+ * at src/KernelFunctions.h:171-175). */
+void D3Q19CudaAaInit_AaSoA(LatticeDesc *ld, KernelData **kernelData, Parameters *params);
+void D3Q19CudaAaDeinit_AaSoA(LatticeDesc *ld, KernelData **kernelData);
+
+/* "cuda-list-aa-pv-soa": AA pattern over the fluid-node list with a push
+ * adjacency. Replaces D3Q19ListAaPvInit_PushSoA / ..Deinit_PushSoA
+ * (src/BenchKernelD3Q19ListAaPv.h, registered at src/KernelFunctions.h:58-62). */
+void D3Q19CudaListAaPvInit_PushSoA(LatticeDesc *ld, KernelData **kernelData, Parameters *params);
+void D3Q19CudaListAaPvDeinit_PushSoA(LatticeDesc *ld, KernelData **kernelData);
+
+/* "cuda-list-pull-split-nt-1s-soa" / "-2s-soa": two-grid pull over the
+ * fluid-node list. Replace D3Q19ListPullSplitNt1SInit_PullSoA,
+ * D3Q19ListPullSplitNt2SInit_PullSoA and D3Q19ListPullSplitNtDeinit_PullSoA
+ * (src/BenchKernelD3Q19ListPullSplitNt.h, src/KernelFunctions.h:96-105). On the
+ * GPU both names run the same one-thread-per-node kernel. */
+void D3Q19CudaListPullSplitNt1SInit_PullSoA(LatticeDesc *ld, KernelData **kernelData, Parameters *params);
+void D3Q19CudaListPullSplitNt2SInit_PullSoA(LatticeDesc *ld, KernelData **kernelData, Parameters *params);
+void D3Q19CudaListPullSplitNtDeinit_PullSoA(LatticeDesc *ld, KernelData **kernelData);
+
+/* The rows above as a table: {Name, Init, Deinit}, in the layout of the
+ * reference's KernelFunctions (src/KernelFunctions.h:49-54). */
+typedef struct LbmB200KernelFunctions_ {
+	char Name[128];
+	void (*Init)(LatticeDesc *ld, KernelData **kernelData, Parameters *params);
+	void (*Deinit)(LatticeDesc *ld, KernelData **kernelData);
+} LbmB200KernelFunctions;
+
+const LbmB200KernelFunctions *lbm_b200_kernels(int *count);
+
+/* ---- host helpers on the same path (src/Kernel.c, src/Geometry.c) ---- */
+
+/* GeoCreateByStr (src/Geometry.c:37-88): box, channel, pipe, blocks[-n],
+ * fluid, and (new) spheres[:seed:porosity:rmin:rmax], see lbm_geo_spheres. Allocates ld->Lattice (free with free()). Periodic flags are recorded
+ * in ld before the geometry forces its own, as in the reference. Returns 0, or
+ * -1 with a message for an unknown geometry or a bad block size. */
+int lbm_geo_create(const char *geometryType, int dims[3], int periodic[3], LatticeDesc *ld);
+
+/* KernelSetInitialDensity / KernelSetInitialVelocity (src/Kernel.c:258-438). */
+void lbm_set_initial_density(LatticeDesc *ld, KernelData *kd, CaseData *cd);
+void lbm_set_initial_velocity(LatticeDesc *ld, KernelData *kd, CaseData *cd);
+
+/* KernelVerifiy (src/Kernel.c:511-625): L2 norm of the relative error of the
+ * x-velocity profile at x = nX/2 against plane Poiseuille flow. Writes
+ * flow-profile.dat into the current directory when write_file is set. */
+double lbm_verify(LatticeDesc *ld, KernelData *kd, CaseData *cd, int write_file);
+
+/* KernelDensity (src/Kernel.c:209-254): mean density over the fluid nodes. */
+double lbm_density(KernelData *kd, LatticeDesc *ld);
+
+/* ---- B200 additions with no counterpart in the reference ---- */
+
+/* Seeded packing of solid spheres in a fully periodic box: random sequential
+ * addition of non-overlapping spheres (radii uniform in [rmin, rmax]) until
+ * the voxel porosity reaches `porosity`, or until `rsaAttempts` placements in
+ * a row have failed (jammed); then spheres are added without the overlap test
+ * until the target is met. Random numbers: splitmix64-seeded PCG32.
+ * stats (optional, 4 doubles): achieved porosity, spheres placed without
+ * overlap, spheres placed with overlap allowed, porosity at jamming (-1 if
+ * the target was reached first). ld gets a malloc'ed mask (free with free())
+ * and periodic flags 1,1,1. Returns 0, or -1 for bad arguments. */
+int lbm_geo_spheres(const int dims[3], uint64_t seed, double porosity, double rmin, double rmax,
+                    int rsaAttempts, LatticeDesc *ld, double *stats);
+
+/* Device time (ms, CUDA events on the kernel's stream) of the time-step loop
+ * of the last Kernel call; Duration holds the host wall time around the same
+ * loop including the final synchronisation. */
+double lbm_b200_last_device_ms(KernelData *kd);
+
+/* Number of kernel launches of the last Kernel call. */
+long lbm_b200_last_launches(KernelData *kd);
+
+/* Bytes moved host->device and device->host by the last Kernel call (mirror
+ * upload of a dirty mirror, download after the steps). */
+void lbm_b200_last_copy_bytes(KernelData *kd, size_t *h2d, size_t *d2h);
+
+/* Runs n time steps without touching the host mirror (no upload, no download,
+ * no synchronisation), for callers that keep the state on the device. Returns
+ * 0, or a CUDA error code. */
+int lbm_b200_step_device(KernelData *kd, CaseData *cd, int n);
+
+/* Copies the device state into the host mirror (blocking). */
+int lbm_b200_sync_mirror(KernelData *kd);
+
+/* Marks the host mirror as changed, so the next Kernel call uploads it. */
+void lbm_b200_mark_mirror_dirty(KernelData *kd);
+
+/* Runs n time steps on the device and times them with CUDA events on the
+ * instance's stream: *total_ms for the whole sequence, per_launch_ms[k]
+ * (optional, n entries) for launch k. No mirror traffic. Returns 0 or a CUDA
+ * error code. */
+int lbm_b200_time_steps(KernelData *kd, CaseData *cd, int n, double *total_ms, double *per_launch_ms);
+
+/* Selects the CUDA device used by subsequent Init calls of this thread. */
+int lbm_b200_set_device(int device);
+
+/* Last CUDA error string seen by the library ("" if none). */
+const char *lbm_b200_last_error(void);
+
+/* Logical PDFs of every fluid cell through GetNode / SetNode: 19 doubles per
+ * lattice cell, cells x fastest (src/Lattice.h:60-76), obstacle cells skipped. */
+void lbm_b200_get_field(KernelData *kd, LatticeDesc *ld, double *out);
+void lbm_b200_set_field(KernelData *kd, LatticeDesc *ld, const double *in);
+
+/* Host-built list layout of a list-kernel instance: fluid-node numbering
+ * (nX*nY*nZ entries, obstacles 0xffffffff), adjacency (nFluid*18, the
+ * reference's order and index encoding), node and padded cell counts.
+ * Returns -1 for the full-array kernel. */
+int lbm_b200_list_layout(KernelData *kd, const uint32_t **grid, const uint32_t **adj, int *nFluid, int *nCells);
+
+/* Host layout builders (no GPU needed), exported for the parity tests:
+ * SoA padding (src/Padding.c:195-244), list numbering + adjacency
+ * (src/BenchKernelD3Q19ListAaPvCommon.c:587-792; pull variant
+ * src/BenchKernelD3Q19ListPullSplitNtCommon.c:548-755). */
+int lbmh_pad_cells(int nCells, int pdfBytes, const char *padStr);
+int lbmh_list_build(const LatticeDesc *ld, int pull, const int blk[3], int nCells,
+                    uint32_t *grid, uint32_t *coords, uint32_t *adj);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBM_B200_H */

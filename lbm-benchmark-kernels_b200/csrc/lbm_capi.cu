@@ -1,0 +1,599 @@
+// lbm_capi.cu -- the C ABI of the B200 kernels: Init/Deinit pairs with the
+// reference's KernelFunctions signatures, the KernelData callbacks they
+// install, and a few flat helpers (include/lbm_b200.h).
+//
+// Device state per kernel instance:
+//   AA full array   one PDF array (19 planes of the padded ghost-layer grid) and
+//                   one uint32 link word per cell;
+//   list AA         one PDF array (19 planes of nCells) and the push adjacency;
+//   list pull       two PDF arrays and the pull adjacency.
+// The host keeps a pinned mirror of the current PDF array for
+// GetNode/SetNode; Kernel uploads it when SetNode has touched it, runs the time
+// steps back to back on the instance's stream, and downloads it afterwards.
+#include <cerrno>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <strings.h>
+
+#include "../../include/lbm_b200.h"
+#include "lbm_host.h"
+#include "lbm_kernels.cuh"
+
+namespace {
+
+using lbm::Q;
+using lbm::QM;
+
+enum Kind { kAa = 0, kListAa = 1, kListPull = 2 };
+
+thread_local std::string g_lastError;
+
+struct Gpu {
+  KernelData kd;  // first member: the reference's KernelData layout
+  Kind kind;
+  int dims[3];
+  int per[3];
+  double lambda;
+  int iteration;  // logical view: -1 before the first step, then the last step done
+
+  // pinned host mirror of the current PDF array
+  double* mirror;
+  size_t mirrorElems;
+  bool dirty;
+
+  // device memory
+  double* dF;
+  double* dG;
+  uint32_t* dLink;
+  uint32_t* dAdj;
+  int* dErr;
+  cudaStream_t stream;
+  cudaEvent_t ev0, ev1;
+
+  // AA layout
+  int xs, pitch;
+  long long dstride;
+
+  // list layout
+  uint32_t* grid;
+  uint32_t* adjHost;
+  int nFluid, nCells;
+  int cur;  // pull: index of the current grid (0 = dF, 1 = dG)
+
+  // last Kernel call
+  double lastDeviceMs;
+  long lastLaunches;
+  size_t lastH2D, lastD2H;
+};
+
+#define LBM_CK(call)                                                                                 \
+  do {                                                                                               \
+    cudaError_t e_ = (call);                                                                         \
+    if (e_ != cudaSuccess) {                                                                         \
+      g_lastError = std::string(#call) + ": " + cudaGetErrorString(e_);                              \
+      std::printf("ERROR: CUDA: %s (%s:%d)\n", g_lastError.c_str(), __FILE__, __LINE__);            \
+      std::exit(1);                                                                                  \
+    }                                                                                                \
+  } while (0)
+
+void usage() {
+  std::printf("Kernel parameters:\n");
+  std::printf("  [-lambda <v|a/b>] [-blk <n>] [-blk-[xyz] <n>] [-pad auto|no|m+o(,m+o)*] [-bs <n>]\n");
+}
+
+struct Args {
+  double lambda = 1.0 / 12.0;
+  int blk[3] = {0, 0, 0};
+  const char* pad = nullptr;
+};
+
+Args parse_args(Parameters* p) {
+  Args a;
+  if (p == nullptr) return a;
+  for (int i = 0; i < p->nKernelArgs; ++i) {
+    const char* s = p->KernelArgs[i];
+    auto need = [&]() -> const char* {
+      if (i + 1 >= p->nKernelArgs) {
+        std::printf("ERROR: argument %s requires a parameter.\n", s);
+        std::exit(1);
+      }
+      return p->KernelArgs[++i];
+    };
+    if (!std::strcmp(s, "-lambda") || !std::strcmp(s, "--lambda")) {
+      const char* v = need();
+      if (lbmh_parse_fraction(v, &a.lambda) || !(a.lambda > 0.0)) {
+        std::printf("ERROR: -lambda needs a positive number or fraction, got \"%s\".\n", v);
+        std::exit(1);
+      }
+    } else if (!std::strcmp(s, "-blk") || !std::strcmp(s, "--blk")) {
+      int v = (int)std::strtol(need(), nullptr, 0);
+      if (v < 0) { std::printf("ERROR: blocking parameter must be >= 0.\n"); std::exit(1); }
+      a.blk[0] = a.blk[1] = a.blk[2] = v;
+    } else if (!std::strncmp(s, "-blk-", 5) || !std::strncmp(s, "--blk-", 6)) {
+      char axis = s[std::strlen(s) - 1];
+      int v = (int)std::strtol(need(), nullptr, 0);
+      if (v < 0 || axis < 'x' || axis > 'z') { std::printf("ERROR: blocking parameter must be >= 0.\n"); std::exit(1); }
+      a.blk[axis - 'x'] = v;
+    } else if (!std::strcmp(s, "-pad") || !std::strcmp(s, "--pad")) {
+      a.pad = need();
+    } else if (!std::strcmp(s, "-bs") || !std::strcmp(s, "--bs")) {
+      (void)need();  // accepted for command-line compatibility; tiles are fixed per kernel
+    } else if (!std::strcmp(s, "-h") || !std::strcmp(s, "-help") || !std::strcmp(s, "--help")) {
+      usage();
+      std::exit(1);
+    } else {
+      std::printf("ERROR: unknown kernel parameter.\n");
+      usage();
+      std::exit(1);
+    }
+  }
+  return a;
+}
+
+lbm::Trt<double> make_trt(double omega, double lambda, double xforce) {
+  // evaluated as the reference does at the top of its kernels
+  // (src/BenchKernelD3Q19Aa.c:69-88, src/Kernel.c:769-795)
+  lbm::Trt<double> t;
+  t.omegaEven = omega;
+  t.omegaOdd = 1.0 / (0.5 + lambda / (1.0 / omega - 0.5));
+  t.w0 = 1.0 / 3.0;
+  t.w1 = 1.0 / 18.0;
+  t.w2 = 1.0 / 36.0;
+  t.w1x3 = t.w1 * 3.0;
+  t.w1nh = t.w1 * 9.0 / 2.0;
+  t.w2x3 = t.w2 * 3.0;
+  t.w2nh = t.w2 * 9.0 / 2.0;
+  const double w[Q] = {t.w1, t.w1, t.w1, t.w1, t.w2, t.w2, t.w2, t.w2, t.w1, t.w2,
+                       t.w2, t.w2, t.w2, t.w1, t.w2, t.w2, t.w2, t.w2, t.w0};
+  for (int d = 0; d < Q; ++d) t.force[d] = 3.0 * w[d] * lbm::cx(d) * xforce;
+  return t;
+}
+
+// --- logical node view on the mirror ---------------------------------------
+
+inline double* slot(Gpu* g, int x, int y, int z, int d) {
+  if (g->kind == kAa) {
+    long c = (long)(x + 1) * g->xs + (long)(y + 1) * g->pitch + z + lbm::kZOff;
+    return g->mirror + d * g->dstride + c;
+  }
+  uint32_t node = g->grid[lbmh_lidx(g->dims, x, y, z)];
+  return g->mirror + (size_t)d * g->nCells + node;
+}
+
+void check_node(Gpu* g, int x, int y, int z) {
+  if (x < 0 || y < 0 || z < 0 || x >= g->dims[0] || y >= g->dims[1] || z >= g->dims[2]) {
+    std::printf("ERROR: node (%d, %d, %d) outside the lattice.\n", x, y, z);
+    std::exit(1);
+  }
+  if (g->kind != kAa && g->grid[lbmh_lidx(g->dims, x, y, z)] == 0xffffffffu) {
+    std::printf("ERROR: node (%d, %d, %d) is an obstacle and has no PDFs in a list layout.\n", x, y, z);
+    std::exit(1);
+  }
+}
+
+// The device state is kept in the reference's natural layout between Kernel
+// calls: the AA kernels always finish an even/odd pair and the pull kernel
+// writes the natural layout every step, so GetNode/SetNode read slot (x, d).
+void cb_get_node(KernelData* kd, int x, int y, int z, PdfT* pdfs) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  check_node(g, x, y, z);
+  for (int d = 0; d < Q; ++d) pdfs[d] = *slot(g, x, y, z, d);
+}
+
+void cb_set_node(KernelData* kd, int x, int y, int z, PdfT* pdfs) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  check_node(g, x, y, z);
+  for (int d = 0; d < Q; ++d) *slot(g, x, y, z, d) = pdfs[d];
+  g->dirty = true;
+}
+
+void cb_bc_get(KernelData* kd, int x, int y, int z, int dir, PdfT* pdf) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  check_node(g, x, y, z);
+  *pdf = *slot(g, x, y, z, dir);
+}
+
+void cb_bc_set(KernelData* kd, int x, int y, int z, int dir, PdfT pdf) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  check_node(g, x, y, z);
+  *slot(g, x, y, z, dir) = pdf;
+  g->dirty = true;
+}
+
+// --- device steps -------------------------------------------------------------
+
+lbm::AaArgs aa_args(Gpu* g) {
+  lbm::AaArgs a;
+  a.f = g->dF;
+  a.dstride = g->dstride;
+  a.link = g->dLink;
+  a.nX = g->dims[0];
+  a.nY = g->dims[1];
+  a.nZ = g->dims[2];
+  a.xs = g->xs;
+  a.pitch = g->pitch;
+  a.perX = g->per[0];
+  a.perY = g->per[1];
+  a.perZ = g->per[2];
+  return a;
+}
+
+lbm::ListArgs list_args(Gpu* g) {
+  lbm::ListArgs a;
+  a.f = g->cur == 0 ? g->dF : g->dG;
+  a.g = g->cur == 0 ? g->dG : g->dF;
+  a.adj = g->dAdj;
+  a.nCells = g->nCells;
+  a.nFluid = g->nFluid;
+  a.err = g->dErr;
+  return a;
+}
+
+double* current_grid(Gpu* g) { return (g->kind == kListPull && g->cur == 1) ? g->dG : g->dF; }
+
+// Enqueues n time steps (AA kernels: rounded up to whole even/odd pairs, as
+// the reference's loop `for (iter = 0; iter < n; iter += 2)`); returns the
+// number of launches. With `ev`, event k is recorded before launch k and one
+// more after the last launch.
+long enqueue_steps(Gpu* g, const lbm::Trt<double>& t, int n, cudaEvent_t* ev = nullptr) {
+  long k = 0;
+  auto mark = [&]() {
+    if (ev) cudaEventRecord(ev[k], g->stream);
+  };
+  if (g->kind == kAa) {
+    lbm::AaArgs a = aa_args(g);
+    for (int it = 0; it < n; it += 2) {
+      mark();
+      lbm::aa_even_fp64(a, t, g->stream);
+      ++k;
+      mark();
+      lbm::aa_odd_fp64(a, t, g->stream);
+      ++k;
+      g->iteration = it + 1;
+    }
+  } else if (g->kind == kListAa) {
+    lbm::ListArgs a = list_args(g);
+    for (int it = 0; it < n; it += 2) {
+      mark();
+      lbm::list_even_fp64(a, t, g->stream);
+      ++k;
+      mark();
+      lbm::list_odd_fp64(a, t, g->stream);
+      ++k;
+      g->iteration = it + 1;
+    }
+  } else {
+    for (int it = 0; it < n; ++it) {
+      lbm::ListArgs a = list_args(g);
+      mark();
+      lbm::list_pull_fp64(a, t, g->stream);
+      ++k;
+      g->cur ^= 1;
+      g->iteration = it;
+    }
+  }
+  mark();
+  return k;
+}
+
+long launches_for(const Gpu* g, int n) { return g->kind == kListPull ? n : 2L * ((n + 1) / 2); }
+
+void upload_if_dirty(Gpu* g) {
+  g->lastH2D = 0;
+  if (!g->dirty) return;
+  LBM_CK(cudaMemcpyAsync(current_grid(g), g->mirror, g->mirrorElems * sizeof(double), cudaMemcpyHostToDevice,
+                         g->stream));
+  g->lastH2D = g->mirrorElems * sizeof(double);
+  g->dirty = false;
+}
+
+void download(Gpu* g) {
+  LBM_CK(cudaMemcpyAsync(g->mirror, current_grid(g), g->mirrorElems * sizeof(double), cudaMemcpyDeviceToHost,
+                         g->stream));
+  LBM_CK(cudaStreamSynchronize(g->stream));
+  g->lastD2H = g->mirrorElems * sizeof(double);
+}
+
+void check_device_error(Gpu* g) {
+  int err = 0;
+  LBM_CK(cudaMemcpy(&err, g->dErr, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    g_lastError = "a device wait exceeded its limit (error word " + std::to_string(err) + ")";
+    std::printf("ERROR: %s\n", g_lastError.c_str());
+    std::exit(1);
+  }
+}
+
+void cb_kernel(LatticeDesc* ld, KernelData* kd, CaseData* cd) {
+  (void)ld;
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (!(cd->Omega > 0.0 && cd->Omega < 2.0)) {
+    std::printf("ERROR: omega must lie in (0, 2).\n");
+    std::exit(1);
+  }
+  upload_if_dirty(g);
+  const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
+
+  LBM_CK(cudaStreamSynchronize(g->stream));
+  auto w0 = std::chrono::steady_clock::now();
+  LBM_CK(cudaEventRecord(g->ev0, g->stream));
+  g->lastLaunches = enqueue_steps(g, t, cd->MaxIterations);
+  LBM_CK(cudaGetLastError());
+  LBM_CK(cudaEventRecord(g->ev1, g->stream));
+  LBM_CK(cudaStreamSynchronize(g->stream));
+  auto w1 = std::chrono::steady_clock::now();
+  float ms = 0.f;
+  LBM_CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+  g->lastDeviceMs = ms;
+  kd->Duration = std::chrono::duration<double>(w1 - w0).count();
+  check_device_error(g);
+  download(g);
+}
+
+// --- Init / Deinit ----------------------------------------------------------------
+
+Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params) {
+  Gpu* g = static_cast<Gpu*>(std::calloc(1, sizeof(Gpu)));
+  if (!g) { std::printf("ERROR: allocation failed.\n"); std::exit(1); }
+  Args a = parse_args(params);
+  g->kind = kind;
+  g->lambda = a.lambda;
+  g->iteration = -1;
+  for (int i = 0; i < 3; ++i) g->dims[i] = ld->Dims[i];
+  g->per[0] = ld->PeriodicX;
+  g->per[1] = ld->PeriodicY;
+  g->per[2] = ld->PeriodicZ;
+  LBM_CK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+  LBM_CK(cudaEventCreate(&g->ev0));
+  LBM_CK(cudaEventCreate(&g->ev1));
+  LBM_CK(cudaMalloc(&g->dErr, sizeof(int)));
+  LBM_CK(cudaMemset(g->dErr, 0, sizeof(int)));
+
+  KernelData* kd = &g->kd;
+  kd->Dims[0] = ld->Dims[0];
+  kd->Dims[1] = ld->Dims[1];
+  kd->Dims[2] = ld->Dims[2];
+  kd->GetNode = cb_get_node;
+  kd->SetNode = cb_set_node;
+  kd->BoundaryConditionsGetPdf = cb_bc_get;
+  kd->BoundaryConditionsSetPdf = cb_bc_set;
+  kd->Kernel = cb_kernel;
+
+  const uint64_t nPdfs = 19ull * ld->Dims[0] * ld->Dims[1] * ld->Dims[2];
+  if (nPdfs >= (1ull << 32)) {
+    std::printf("ERROR: number of PDFs exceeds the 32-bit indices of this layout.\n");
+    std::exit(1);
+  }
+
+  if (kind == kAa) {
+    const int gx = ld->Dims[0] + 2, gy = ld->Dims[1] + 2;
+    g->pitch = (ld->Dims[2] + lbm::kZOff + 1 + 3) / 4 * 4;
+    g->xs = gy * g->pitch;
+    g->dstride = (long long)gx * g->xs;
+    g->mirrorElems = (size_t)Q * g->dstride;
+    kd->GlobalDims[0] = gx;
+    kd->GlobalDims[1] = gy;
+    kd->GlobalDims[2] = ld->Dims[2] + 2;
+    kd->Offsets[0] = kd->Offsets[1] = kd->Offsets[2] = 1;
+    kd->LoopBalance = 2.0 * 19 * sizeof(double);
+
+    uint32_t* link = static_cast<uint32_t*>(std::malloc(sizeof(uint32_t) * (size_t)g->dstride));
+    if (!link) { std::printf("ERROR: allocation failed.\n"); std::exit(1); }
+    lbmh_aa_links(ld, g->xs, g->pitch, lbm::kZOff, link);
+    LBM_CK(cudaMalloc(&g->dLink, sizeof(uint32_t) * (size_t)g->dstride));
+    LBM_CK(cudaMemcpy(g->dLink, link, sizeof(uint32_t) * (size_t)g->dstride, cudaMemcpyHostToDevice));
+    std::free(link);
+    LBM_CK(cudaMalloc(&g->dF, sizeof(double) * g->mirrorElems));
+    LBM_CK(cudaMemset(g->dF, 0, sizeof(double) * g->mirrorElems));
+  } else {
+    const bool pull = kind == kListPull;
+    int nCells = lbmh_pad_cells(ld->nFluid, (int)sizeof(double), a.pad);
+    if (nCells < 0) std::exit(1);
+    if (pull) nCells = nCells + (8 - nCells % 8);  // cache-line pad (src/BenchKernelD3Q19ListPullSplitNtCommon.c:494-496)
+    g->nCells = nCells;
+    g->nFluid = ld->nFluid;
+    const long ncell = (long)ld->Dims[0] * ld->Dims[1] * ld->Dims[2];
+    g->grid = static_cast<uint32_t*>(std::malloc(sizeof(uint32_t) * ncell));
+    const long nTiles = (g->nFluid + lbm::kListTile - 1) / lbm::kListTile;
+    const size_t adjElems = (size_t)(nTiles > 0 ? nTiles : 1) * lbm::kListTile * QM;
+    g->adjHost = static_cast<uint32_t*>(std::calloc(adjElems, sizeof(uint32_t)));
+    if (!g->grid || !g->adjHost) { std::printf("ERROR: allocation failed.\n"); std::exit(1); }
+    const int nf = lbmh_list_build(ld, pull ? 1 : 0, a.blk, nCells, g->grid, nullptr, g->adjHost);
+    if (nf != g->nFluid) { std::printf("ERROR: fluid node count mismatch.\n"); std::exit(1); }
+    LBM_CK(cudaMalloc(&g->dAdj, sizeof(uint32_t) * adjElems));
+    LBM_CK(cudaMemcpy(g->dAdj, g->adjHost, sizeof(uint32_t) * adjElems, cudaMemcpyHostToDevice));
+    g->mirrorElems = (size_t)Q * nCells;
+    LBM_CK(cudaMalloc(&g->dF, sizeof(double) * g->mirrorElems));
+    LBM_CK(cudaMemset(g->dF, 0, sizeof(double) * g->mirrorElems));
+    if (pull) {
+      LBM_CK(cudaMalloc(&g->dG, sizeof(double) * g->mirrorElems));
+      LBM_CK(cudaMemset(g->dG, 0, sizeof(double) * g->mirrorElems));
+    }
+    kd->GlobalDims[0] = ld->Dims[0];
+    kd->GlobalDims[1] = ld->Dims[1];
+    kd->GlobalDims[2] = ld->Dims[2];
+    // the GPU odd step reads all 18 adjacency entries of a node every time
+    kd->LoopBalance = pull ? 2.0 * 19 * 8 + 18 * 4.0 : (2.0 * 19 * 8 + (2.0 * 19 * 8 + 18 * 4.0)) / 2.0;
+  }
+
+  LBM_CK(cudaMallocHost(&g->mirror, sizeof(double) * g->mirrorElems));
+  std::memset(g->mirror, 0, sizeof(double) * g->mirrorElems);
+  g->dirty = false;  // device and mirror both hold zeros
+  kd->Pdfs[0] = g->mirror;
+  kd->Pdfs[1] = nullptr;
+  kd->PdfsActive = g->mirror;
+  return g;
+}
+
+void gpu_free(KernelData** kernelData) {
+  if (kernelData == nullptr || *kernelData == nullptr) return;
+  Gpu* g = reinterpret_cast<Gpu*>(*kernelData);
+  cudaStreamSynchronize(g->stream);
+  cudaFree(g->dF);
+  cudaFree(g->dG);
+  cudaFree(g->dLink);
+  cudaFree(g->dAdj);
+  cudaFree(g->dErr);
+  cudaFreeHost(g->mirror);
+  cudaEventDestroy(g->ev0);
+  cudaEventDestroy(g->ev1);
+  cudaStreamDestroy(g->stream);
+  std::free(g->grid);
+  std::free(g->adjHost);
+  std::free(g);
+  *kernelData = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+void D3Q19CudaAaInit_AaSoA(LatticeDesc* ld, KernelData** kernelData, Parameters* params) {
+  *kernelData = &gpu_new(kAa, ld, params)->kd;
+}
+void D3Q19CudaAaDeinit_AaSoA(LatticeDesc* ld, KernelData** kernelData) {
+  (void)ld;
+  gpu_free(kernelData);
+}
+
+void D3Q19CudaListAaPvInit_PushSoA(LatticeDesc* ld, KernelData** kernelData, Parameters* params) {
+  *kernelData = &gpu_new(kListAa, ld, params)->kd;
+}
+void D3Q19CudaListAaPvDeinit_PushSoA(LatticeDesc* ld, KernelData** kernelData) {
+  (void)ld;
+  gpu_free(kernelData);
+}
+
+void D3Q19CudaListPullSplitNt1SInit_PullSoA(LatticeDesc* ld, KernelData** kernelData, Parameters* params) {
+  *kernelData = &gpu_new(kListPull, ld, params)->kd;
+}
+void D3Q19CudaListPullSplitNt2SInit_PullSoA(LatticeDesc* ld, KernelData** kernelData, Parameters* params) {
+  *kernelData = &gpu_new(kListPull, ld, params)->kd;
+}
+void D3Q19CudaListPullSplitNtDeinit_PullSoA(LatticeDesc* ld, KernelData** kernelData) {
+  (void)ld;
+  gpu_free(kernelData);
+}
+
+static const LbmB200KernelFunctions kTable[] = {
+    {"cuda-aa-soa", D3Q19CudaAaInit_AaSoA, D3Q19CudaAaDeinit_AaSoA},
+    {"cuda-list-aa-pv-soa", D3Q19CudaListAaPvInit_PushSoA, D3Q19CudaListAaPvDeinit_PushSoA},
+    {"cuda-list-pull-split-nt-1s-soa", D3Q19CudaListPullSplitNt1SInit_PullSoA, D3Q19CudaListPullSplitNtDeinit_PullSoA},
+    {"cuda-list-pull-split-nt-2s-soa", D3Q19CudaListPullSplitNt2SInit_PullSoA, D3Q19CudaListPullSplitNtDeinit_PullSoA},
+};
+
+const LbmB200KernelFunctions* lbm_b200_kernels(int* count) {
+  if (count) *count = (int)(sizeof(kTable) / sizeof(kTable[0]));
+  return kTable;
+}
+
+double lbm_b200_last_device_ms(KernelData* kd) { return reinterpret_cast<Gpu*>(kd)->lastDeviceMs; }
+
+long lbm_b200_last_launches(KernelData* kd) { return reinterpret_cast<Gpu*>(kd)->lastLaunches; }
+
+void lbm_b200_last_copy_bytes(KernelData* kd, size_t* h2d, size_t* d2h) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (h2d) *h2d = g->lastH2D;
+  if (d2h) *d2h = g->lastD2H;
+}
+
+int lbm_b200_step_device(KernelData* kd, CaseData* cd, int n) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (g->dirty) upload_if_dirty(g);
+  const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
+  g->lastLaunches = enqueue_steps(g, t, n);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) g_lastError = cudaGetErrorString(e);
+  return (int)e;
+}
+
+int lbm_b200_sync_mirror(KernelData* kd) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  cudaError_t e = cudaStreamSynchronize(g->stream);
+  if (e != cudaSuccess) { g_lastError = cudaGetErrorString(e); return (int)e; }
+  download(g);
+  return 0;
+}
+
+const char* lbm_b200_last_error(void) { return g_lastError.c_str(); }
+
+void lbm_b200_mark_mirror_dirty(KernelData* kd) { reinterpret_cast<Gpu*>(kd)->dirty = true; }
+
+int lbm_b200_time_steps(KernelData* kd, CaseData* cd, int n, double* total_ms, double* per_launch_ms) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (g->dirty) upload_if_dirty(g);
+  const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
+  const long nl = launches_for(g, n);
+  cudaEvent_t* ev = static_cast<cudaEvent_t*>(std::malloc(sizeof(cudaEvent_t) * (nl + 1)));
+  for (long k = 0; k <= nl; ++k) cudaEventCreate(&ev[k]);
+  cudaError_t e = cudaStreamSynchronize(g->stream);
+  if (e == cudaSuccess) {
+    g->lastLaunches = enqueue_steps(g, t, n, ev);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  if (e == cudaSuccess) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[0], ev[nl]);
+    if (total_ms) *total_ms = ms;
+    if (per_launch_ms)
+      for (long k = 0; k < nl; ++k) {
+        cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+        per_launch_ms[k] = ms;
+      }
+  }
+  for (long k = 0; k <= nl; ++k) cudaEventDestroy(ev[k]);
+  std::free(ev);
+  if (e != cudaSuccess) { g_lastError = cudaGetErrorString(e); return (int)e; }
+  int err = 0;
+  cudaMemcpy(&err, g->dErr, sizeof(int), cudaMemcpyDeviceToHost);
+  if (err) { g_lastError = "a device wait exceeded its limit"; return -1; }
+  return 0;
+}
+
+int lbm_b200_set_device(int device) {
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) g_lastError = cudaGetErrorString(e);
+  return (int)e;
+}
+
+// Bulk access to the logical PDFs of every fluid cell (19 doubles per cell,
+// cells x fastest, obstacle cells skipped), through GetNode/SetNode.
+void lbm_b200_get_field(KernelData* kd, LatticeDesc* ld, double* out) {
+  const int* dims = ld->Dims;
+  for (int z = 0; z < dims[2]; ++z)
+    for (int y = 0; y < dims[1]; ++y)
+      for (int x = 0; x < dims[0]; ++x) {
+        const long c = lbmh_lidx(dims, x, y, z);
+        if (ld->Lattice[c] == LAT_CELL_OBSTACLE) continue;
+        kd->GetNode(kd, x, y, z, out + c * Q);
+      }
+}
+
+void lbm_b200_set_field(KernelData* kd, LatticeDesc* ld, const double* in) {
+  const int* dims = ld->Dims;
+  for (int z = 0; z < dims[2]; ++z)
+    for (int y = 0; y < dims[1]; ++y)
+      for (int x = 0; x < dims[0]; ++x) {
+        const long c = lbmh_lidx(dims, x, y, z);
+        if (ld->Lattice[c] == LAT_CELL_OBSTACLE) continue;
+        kd->SetNode(kd, x, y, z, const_cast<double*>(in + c * Q));
+      }
+}
+
+// The host-built list layout of a list kernel instance (for parity checks):
+// grid (nX*nY*nZ), adjacency (nFluid*18, the reference's order), counts.
+int lbm_b200_list_layout(KernelData* kd, const uint32_t** grid, const uint32_t** adj, int* nFluid, int* nCells) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (g->kind == kAa) return -1;
+  if (grid) *grid = g->grid;
+  if (adj) *adj = g->adjHost;
+  if (nFluid) *nFluid = g->nFluid;
+  if (nCells) *nCells = g->nCells;
+  return 0;
+}
+
+}  // extern "C"

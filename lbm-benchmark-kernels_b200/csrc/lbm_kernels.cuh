@@ -1,0 +1,65 @@
+// lbm_kernels.cuh -- argument blocks and launchers of the sm_100a D3Q19 TRT
+// time-step kernels (definitions in lbm_kernels_fp64.cu).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "lbm_d3q19.cuh"
+
+namespace lbm {
+
+// ---------------------------------------------------------------------------
+// Full-array AA layout on the device.
+//
+// SoA, one plane per direction. Cells carry the reference's one-cell ghost
+// layer ((nX+2) x (nY+2) x (nZ+2), src/BenchKernelD3Q19AaCommon.c:331-337) so
+// that non-periodic fluid faces keep the reference's semantics, but the z rows
+// are padded: interior z = 0 sits at element kZOff of a row whose pitch is a
+// multiple of 4 doubles, so every warp's 32 consecutive z cells start on a 32 B
+// sector boundary.
+//   cell(x, y, z) = (x + 1) * xs + (y + 1) * pitch + z + kZOff   (x,y,z interior coords)
+//   pdf(d, cell)  = f[d * dstride + cell]
+// link[cell] (uint32): bit 31 = fluid cell; bit d (d < 18) = the neighbour
+// x + c_d is not a fluid node reached directly or through a periodic wrap
+// (a wall: bounce back, or an open non-periodic face).
+constexpr int kZOff = 4;
+constexpr uint32_t kFluidBit = 0x80000000u;
+
+struct AaArgs {
+  double* f;
+  long long dstride;
+  const uint32_t* link;
+  int nX, nY, nZ;
+  int xs, pitch;
+  int perX, perY, perZ;
+};
+
+// ---------------------------------------------------------------------------
+// Fluid-node list layout (the reference's list kernels).
+//   pdf(d, n) = f[d * nCells + n], nCells = padded cell count
+//   adj[n * 18 + d] = PDF index (d' * nCells + m) of link d of node n, push or
+//   pull as in src/BenchKernelD3Q19ListAaPvCommon.c:700-792 /
+//   src/BenchKernelD3Q19ListPullSplitNtCommon.c:662-755.
+// The adjacency allocation holds whole tiles of kListTile nodes so that every
+// tile can be fetched with one bulk copy.
+constexpr int kListTile = 256;
+
+struct ListArgs {
+  double* f;      // list AA: the one grid; pull: source grid
+  double* g;      // pull: destination grid
+  const uint32_t* adj;
+  long long nCells;
+  int nFluid;
+  int* err;       // device error word (bounded waits)
+};
+
+// Launchers (stream-ordered, no synchronisation).
+void aa_even_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
+void aa_odd_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
+void list_even_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
+void list_odd_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
+void list_pull_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
+
+}  // namespace lbm

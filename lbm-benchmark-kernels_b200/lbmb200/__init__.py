@@ -1,0 +1,294 @@
+"""Python mirror of the reference benchmark's kernel-table API over the B200
+C ABI (include/lbm_b200.h, liblbmb200.so).
+
+The flow is the one src/Main.c follows::
+
+    ld = geometry("box", (16, 16, 16), periodic=(1, 1, 0))     # GeoCreateByStr
+    kf = kernel("cuda-aa-soa")                                  # g_kernels lookup
+    kd = kf.init(ld, kernel_args=["-lambda", "3/16"])           # kf->Init
+    kd.set_initial_density(cd); kd.set_initial_velocity(cd)     # -verify init
+    kd.run(cd)                                                  # kd->Kernel
+    err = kd.verify(cd)                                         # KernelVerifiy
+    kd.deinit()                                                 # kf->Deinit
+
+Kernel names follow the reference's (src/KernelFunctions.h:56-188) with a
+"cuda-" prefix; lookups are case-insensitive as in src/Main.c:543. There is no
+CPU fallback: loading fails loudly when the library is missing, and running a
+kernel without a GPU fails in the CUDA runtime.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "liblbmb200.so")
+
+Q = 19
+W = np.array([1 / 18] * 4 + [1 / 36] * 4 + [1 / 18] + [1 / 36] * 4 + [1 / 18] + [1 / 36] * 4 + [1 / 3])
+
+
+class LatticeDesc(ctypes.Structure):
+    _fields_ = [("Dims", ctypes.c_int * 3), ("Lattice", ctypes.POINTER(ctypes.c_int)),
+                ("nCells", ctypes.c_int), ("nFluid", ctypes.c_int), ("nObst", ctypes.c_int),
+                ("nInlet", ctypes.c_int), ("nOutlet", ctypes.c_int), ("PeriodicX", ctypes.c_int),
+                ("PeriodicY", ctypes.c_int), ("PeriodicZ", ctypes.c_int), ("Name", ctypes.c_char_p)]
+
+
+class CaseData(ctypes.Structure):
+    _fields_ = [("Omega", ctypes.c_double), ("RhoIn", ctypes.c_double), ("RhoOut", ctypes.c_double),
+                ("Ux", ctypes.c_double), ("Uy", ctypes.c_double), ("Uz", ctypes.c_double),
+                ("XForce", ctypes.c_double), ("MaxIterations", ctypes.c_int), ("VtkOutput", ctypes.c_int),
+                ("VtkModulus", ctypes.c_int), ("StatisticsModulus", ctypes.c_int)]
+
+
+class KernelData(ctypes.Structure):
+    pass
+
+
+_GETNODE = ctypes.CFUNCTYPE(None, ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                            ctypes.POINTER(ctypes.c_double))
+_KERNEL = ctypes.CFUNCTYPE(None, ctypes.POINTER(LatticeDesc), ctypes.POINTER(KernelData),
+                           ctypes.POINTER(CaseData))
+_BCGET = ctypes.CFUNCTYPE(None, ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                          ctypes.c_int, ctypes.POINTER(ctypes.c_double))
+_BCSET = ctypes.CFUNCTYPE(None, ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                          ctypes.c_int, ctypes.c_double)
+
+KernelData._fields_ = [
+    ("Pdfs", ctypes.POINTER(ctypes.c_double) * 2), ("SrcPdfs", ctypes.POINTER(ctypes.c_double)),
+    ("DstPdfs", ctypes.POINTER(ctypes.c_double)), ("PdfsActive", ctypes.POINTER(ctypes.c_double)),
+    ("Dims", ctypes.c_int * 3), ("GlobalDims", ctypes.c_int * 3), ("Offsets", ctypes.c_int * 3),
+    ("ObstIndices", ctypes.POINTER(ctypes.c_int)), ("nObstIndices", ctypes.c_int),
+    ("BounceBackPdfsSrc", ctypes.POINTER(ctypes.c_int)), ("BounceBackPdfsDst", ctypes.POINTER(ctypes.c_int)),
+    ("nBounceBackPdfs", ctypes.c_int), ("LoopBalance", ctypes.c_double), ("Duration", ctypes.c_double),
+    ("BoundaryConditionsGetPdf", _BCGET), ("BoundaryConditionsSetPdf", _BCSET),
+    ("GetNode", _GETNODE), ("SetNode", _GETNODE), ("Kernel", _KERNEL)]
+
+
+class Parameters(ctypes.Structure):
+    _fields_ = [("nArgs", ctypes.c_int), ("Args", ctypes.POINTER(ctypes.c_char_p)),
+                ("nKernelArgs", ctypes.c_int), ("KernelArgs", ctypes.POINTER(ctypes.c_char_p))]
+
+
+_INIT = ctypes.CFUNCTYPE(None, ctypes.POINTER(LatticeDesc), ctypes.POINTER(ctypes.POINTER(KernelData)),
+                         ctypes.POINTER(Parameters))
+_DEINIT = ctypes.CFUNCTYPE(None, ctypes.POINTER(LatticeDesc), ctypes.POINTER(ctypes.POINTER(KernelData)))
+
+
+class _KF(ctypes.Structure):
+    _fields_ = [("Name", ctypes.c_char * 128), ("Init", _INIT), ("Deinit", _DEINIT)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded liblbmb200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("liblbmb200.so is not built (run: make -C lbm-benchmark-kernels_b200)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.lbm_b200_kernels.restype = ctypes.POINTER(_KF)
+        L.lbm_b200_kernels.argtypes = [ctypes.POINTER(ctypes.c_int)]
+        L.lbm_b200_last_device_ms.restype = ctypes.c_double
+        L.lbm_b200_last_launches.restype = ctypes.c_long
+        L.lbm_b200_last_error.restype = ctypes.c_char_p
+        L.lbm_verify.restype = ctypes.c_double
+        L.lbm_density.restype = ctypes.c_double
+        L.lbm_geo_create.argtypes = [ctypes.c_char_p, ctypes.c_int * 3, ctypes.c_int * 3,
+                                     ctypes.POINTER(LatticeDesc)]
+        _lib = L
+    return _lib
+
+
+def kernel_names():
+    n = ctypes.c_int(0)
+    t = lib().lbm_b200_kernels(ctypes.byref(n))
+    return [t[i].Name.decode() for i in range(n.value)]
+
+
+class Lattice:
+    """A LatticeDesc plus the numpy array that owns its mask."""
+
+    def __init__(self, mask, dims, periodic, name="custom"):
+        self.mask = np.ascontiguousarray(mask, dtype=np.int32).reshape(-1)
+        self.dims = tuple(int(v) for v in dims)
+        assert self.mask.size == self.dims[0] * self.dims[1] * self.dims[2]
+        self._name = name.encode()
+        d = LatticeDesc()
+        for i in range(3):
+            d.Dims[i] = self.dims[i]
+        d.Lattice = self.mask.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        d.nCells = int(self.mask.size)
+        d.nObst = int(np.count_nonzero(self.mask == 0))
+        d.nFluid = int(self.mask.size - d.nObst)
+        d.nInlet = int(np.count_nonzero(self.mask == 2))
+        d.nOutlet = int(np.count_nonzero(self.mask == 4))
+        d.PeriodicX, d.PeriodicY, d.PeriodicZ = (int(v) for v in periodic)
+        d.Name = self._name
+        self.desc = d
+
+    @property
+    def periodic(self):
+        return (self.desc.PeriodicX, self.desc.PeriodicY, self.desc.PeriodicZ)
+
+    @property
+    def n_fluid(self):
+        return self.desc.nFluid
+
+
+def geometry(name, dims, periodic=(0, 0, 0)):
+    """GeoCreateByStr through the library (src/Geometry.c:37-281)."""
+    d = (ctypes.c_int * 3)(*dims)
+    p = (ctypes.c_int * 3)(*periodic)
+    ld = LatticeDesc()
+    rc = lib().lbm_geo_create(name.encode(), d, p, ctypes.byref(ld))
+    if rc != 0:
+        raise ValueError("geometry %r rejected" % name)
+    n = dims[0] * dims[1] * dims[2]
+    mask = np.ctypeslib.as_array(ld.Lattice, shape=(n,)).copy()
+    ctypes.CDLL(None).free(ctypes.cast(ld.Lattice, ctypes.c_void_p))
+    lat = Lattice(mask, dims, (ld.PeriodicX, ld.PeriodicY, ld.PeriodicZ), ld.Name.decode())
+    lat.geo_periodic = tuple(p)  # the flags after the geometry forced its own
+    return lat
+
+
+def case(omega=1.0, xforce=1e-5, iterations=10, rho_in=1.0, rho_out=1.0):
+    cd = CaseData()
+    cd.Omega, cd.XForce, cd.MaxIterations = omega, xforce, iterations
+    cd.RhoIn, cd.RhoOut = rho_in, rho_out
+    cd.VtkModulus = cd.StatisticsModulus = 100
+    return cd
+
+
+class Kernel:
+    """One row of the kernel table: {Name, Init, Deinit}."""
+
+    def __init__(self, row):
+        self.name = row.Name.decode()
+        self._row = row
+
+    def init(self, lattice, kernel_args=()):
+        args = [a.encode() for a in kernel_args]
+        arr = (ctypes.c_char_p * max(1, len(args)))(*args)
+        p = Parameters(0, None, len(args), arr)
+        kdp = ctypes.POINTER(KernelData)()
+        self._row.Init(ctypes.byref(lattice.desc), ctypes.byref(kdp), ctypes.byref(p))
+        return Instance(self, lattice, kdp)
+
+
+def kernel(name):
+    n = ctypes.c_int(0)
+    t = lib().lbm_b200_kernels(ctypes.byref(n))
+    for i in range(n.value):
+        if t[i].Name.decode().lower() == name.lower():
+            return Kernel(t[i])
+    raise KeyError("requested kernel %r not found; available: %s" % (name, ", ".join(kernel_names())))
+
+
+class Instance:
+    """An initialised kernel (the KernelData an Init returned)."""
+
+    def __init__(self, kf, lattice, kdp):
+        self.kf, self.lattice, self.kdp = kf, lattice, kdp
+
+    @property
+    def kd(self):
+        return self.kdp.contents
+
+    def set_initial_density(self, cd):
+        lib().lbm_set_initial_density(ctypes.byref(self.lattice.desc), self.kdp, ctypes.byref(cd))
+
+    def set_initial_velocity(self, cd):
+        lib().lbm_set_initial_velocity(ctypes.byref(self.lattice.desc), self.kdp, ctypes.byref(cd))
+
+    def run(self, cd):
+        """kd->Kernel: cd.MaxIterations steps; returns the kernel's Duration."""
+        self.kd.Kernel(ctypes.byref(self.lattice.desc), self.kdp, ctypes.byref(cd))
+        return self.kd.Duration
+
+    def step_device(self, cd, n):
+        rc = lib().lbm_b200_step_device(self.kdp, ctypes.byref(cd), int(n))
+        if rc:
+            raise RuntimeError(lib().lbm_b200_last_error().decode())
+
+    def sync_mirror(self):
+        rc = lib().lbm_b200_sync_mirror(self.kdp)
+        if rc:
+            raise RuntimeError(lib().lbm_b200_last_error().decode())
+
+    def get_node(self, x, y, z):
+        out = (ctypes.c_double * Q)()
+        self.kd.GetNode(self.kdp, x, y, z, out)
+        return np.array(out[:])
+
+    def set_node(self, x, y, z, pdfs):
+        arr = (ctypes.c_double * Q)(*[float(v) for v in pdfs])
+        self.kd.SetNode(self.kdp, x, y, z, arr)
+
+    def get_field(self):
+        out = np.full(self.lattice.mask.size * Q, np.nan)
+        lib().lbm_b200_get_field(self.kdp, ctypes.byref(self.lattice.desc),
+                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out.reshape(-1, Q)
+
+    def set_field(self, pdfs):
+        pdfs = np.ascontiguousarray(pdfs, dtype=np.float64).reshape(-1)
+        lib().lbm_b200_set_field(self.kdp, ctypes.byref(self.lattice.desc),
+                                 pdfs.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+
+    def verify(self, cd, write_file=False):
+        return lib().lbm_verify(ctypes.byref(self.lattice.desc), self.kdp, ctypes.byref(cd), int(write_file))
+
+    def density(self):
+        return lib().lbm_density(self.kdp, ctypes.byref(self.lattice.desc))
+
+    def list_layout(self):
+        g = ctypes.POINTER(ctypes.c_uint32)()
+        a = ctypes.POINTER(ctypes.c_uint32)()
+        nf, nc = ctypes.c_int(0), ctypes.c_int(0)
+        rc = lib().lbm_b200_list_layout(self.kdp, ctypes.byref(g), ctypes.byref(a), ctypes.byref(nf),
+                                        ctypes.byref(nc))
+        if rc:
+            raise ValueError("not a list kernel")
+        grid = np.ctypeslib.as_array(g, shape=(self.lattice.mask.size,)).copy()
+        adj = np.ctypeslib.as_array(a, shape=(max(nf.value, 1) * 18,))[: nf.value * 18].copy()
+        return grid, adj, nf.value, nc.value
+
+    @property
+    def last_device_ms(self):
+        return lib().lbm_b200_last_device_ms(self.kdp)
+
+    @property
+    def last_launches(self):
+        return lib().lbm_b200_last_launches(self.kdp)
+
+    def last_copy_bytes(self):
+        h, d = ctypes.c_size_t(0), ctypes.c_size_t(0)
+        lib().lbm_b200_last_copy_bytes(self.kdp, ctypes.byref(h), ctypes.byref(d))
+        return h.value, d.value
+
+    def deinit(self):
+        if self.kdp:
+            self.kf._row.Deinit(ctypes.byref(self.lattice.desc), ctypes.byref(self.kdp))
+            self.kdp = ctypes.POINTER(KernelData)()
+
+
+def list_build(lattice, pull, blk=(0, 0, 0), pad=None):
+    """Host list layout without a GPU: (grid, adj, nFluid, nCells)."""
+    L = lib()
+    n_cells = L.lbmh_pad_cells(lattice.n_fluid, 8, pad.encode() if pad else None)
+    if n_cells < 0:
+        raise ValueError("bad padding string %r" % pad)
+    if pull:
+        n_cells = n_cells + (8 - n_cells % 8)
+    grid = np.zeros(lattice.mask.size, dtype=np.uint32)
+    adj = np.zeros(max(lattice.n_fluid, 1) * 18, dtype=np.uint32)
+    b = (ctypes.c_int * 3)(*blk)
+    nf = L.lbmh_list_build(ctypes.byref(lattice.desc), int(bool(pull)), b, n_cells,
+                           grid.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), None,
+                           adj.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+    return grid, adj[: nf * 18], nf, n_cells
