@@ -212,7 +212,8 @@ def time_kernel(lbmb200, kname, lat, steps, warmup, kargs, dist, odd_key):
             rc = L.lbm_b200_time_steps(inst.kdp, ctypes.byref(cd), warmup, ctypes.byref(tot), None)
             if rc:
                 raise RuntimeError(L.lbm_b200_last_error().decode())
-        n_launch = steps if "pull" in kname else 2 * ((steps + 1) // 2)
+        per_pair = 3 if (kname == "cuda-aa-soa" and min(lat.dims) > 2) else 2
+        n_launch = steps if "pull" in kname else per_pair * ((steps + 1) // 2)
         per = (ctypes.c_double * n_launch)()
         dist.barrier()
         rc = L.lbm_b200_time_steps(inst.kdp, ctypes.byref(cd), steps, ctypes.byref(tot), per)
@@ -220,7 +221,8 @@ def time_kernel(lbmb200, kname, lat, steps, warmup, kargs, dist, odd_key):
             raise RuntimeError(L.lbm_b200_last_error().decode())
         dist.barrier()
         per = list(per)
-        res = {"ms": tot.value, "launches": n_launch, "steps_run": n_launch if "pull" in kname else n_launch,
+        res = {"ms": tot.value, "launches": n_launch,
+               "steps_run": n_launch if "pull" in kname else 2 * ((steps + 1) // 2),
                "per_launch_ms": per, "inst": inst}
         return res
     except Exception:
@@ -340,7 +342,7 @@ def run_ours(args, dist):
 
     nf_total = dist.sum(lat.n_fluid)
     ms = dist.max(t["ms"])
-    steps_run = t["launches"]
+    steps_run = t["steps_run"]
     value = nf_total * steps_run / (ms / 1e3) / 1e6
     per = t["per_launch_ms"]
     even = per[0::2]
@@ -370,7 +372,7 @@ def run_ours(args, dist):
         "e2e": {"value": round(nf_total * e2e_iters / e2e_s / 1e6, 3), "unit": "MFLUP/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "step": "one Kernel() call of 500 time steps with PDF upload and download"},
-        "gpu_launches": steps_run,
+        "gpu_launches": t["launches"],
         "clocks": clk,
     }
 
@@ -389,15 +391,30 @@ def run_ours(args, dist):
         fl = lbmb200.geometry("fluid", (args.edge,) * 3, (1, 1, 1))
         ta = time_kernel(lbmb200, "cuda-aa-soa", fl, min(args.steps, 200), 4, kargs, dist, "aa")
         ta["inst"].deinit()
-        am = statistics.mean(ta["per_launch_ms"])
-        ev = statistics.mean(ta["per_launch_ms"][0::2])
-        od = statistics.mean(ta["per_launch_ms"][1::2])
+        per = ta["per_launch_ms"]  # per pair: even, odd interior, odd face shell
+        ev = statistics.mean(per[0::3])
+        od = statistics.mean([a + b for a, b in zip(per[1::3], per[2::3])])
+        am = (ev + od) / 2
         extra["cuda-aa-soa"] = {
             "workload": "%d^3 fully periodic fluid box" % args.edge, "fluid_nodes": fl.n_fluid,
             "mflups": round(fl.n_fluid / (am / 1e3) / 1e6, 1),
             "achieved_gbs": round(B_PER_FLUP["aa"] * fl.n_fluid / (am / 1e3) / 1e9, 1),
             "frac": round(B_PER_FLUP["aa"] * fl.n_fluid / (am / 1e3) / 1e9 / peak, 4),
-            "even_ms": round(ev, 5), "odd_ms": round(od, 5)}
+            "even_ms": round(ev, 5), "odd_ms": round(od, 5),
+            "odd_face_ms": round(statistics.mean(per[2::3]), 5)}
+        # reduced storage list AA on the porous domain (FP32 arithmetic)
+        for prec, pb in (("fp32", 4), ("fp16", 2)):
+            tl = time_kernel(lbmb200, "cuda-list-aa-pv-soa", lat, min(args.steps, 200), 4,
+                             kargs + ["-precision", prec], dist, "odd")
+            tl["inst"].deinit()
+            m = statistics.mean(tl["per_launch_ms"])
+            bpf = 2 * 19 * pb + 36
+            extra["cuda-list-aa-pv-soa/" + prec] = {
+                "mflups": round(lat.n_fluid / (m / 1e3) / 1e6, 1), "bytes_per_flup": bpf,
+                "achieved_gbs": round(bpf * lat.n_fluid / (m / 1e3) / 1e9, 1),
+                "frac": round(bpf * lat.n_fluid / (m / 1e3) / 1e9 / peak, 4),
+                "even_ms": round(statistics.mean(tl["per_launch_ms"][0::2]), 5),
+                "odd_ms": round(statistics.mean(tl["per_launch_ms"][1::2]), 5)}
         line["kernels"] = extra
 
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu:

@@ -207,6 +207,20 @@ int lbm_b200_time_steps(KernelData *kd, CaseData *cd, int n, double *total_ms, d
 /* Selects the CUDA device used by subsequent Init calls of this thread. */
 int lbm_b200_set_device(int device);
 
+/* Device state of a list-kernel instance: the current PDF array (list
+ * layout, f[d * nCells + n]), its padded cell count and node count, and the
+ * instance's CUDA stream. Returns -1 for the full-array kernel. */
+int lbm_b200_device_state(KernelData *kd, double **pdfs, long long *nCells, int *nFluid, void **stream);
+
+/* FP64 conservation sums over the fluid nodes of a list-layout PDF array on
+ * the device: out_device[0..3] = {sum rho, sum j_x, sum j_y, sum j_z}, with
+ * rho = sum_i f_i and j = sum_i c_i f_i per node (the sums KernelDensity and
+ * KernelStatisticsAdv form through GetNode, src/Kernel.c:209-254,633-755).
+ * Fixed reduction tree: the result depends only on the field. Allocates a
+ * scratch of 4 doubles per 256 nodes with cudaMalloc; stream may be NULL.
+ * Synchronises the stream. Returns 0, or a CUDA error code / -1. */
+int lbm_b200_moments_device(const double *pdfs, long long nCells, int nFluid, double *out_device, void *stream);
+
 /* Last CUDA error string seen by the library ("" if none). */
 const char *lbm_b200_last_error(void);
 

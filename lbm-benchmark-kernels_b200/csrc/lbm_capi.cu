@@ -39,10 +39,13 @@ struct Gpu {
   double lambda;
   int iteration;  // logical view: -1 before the first step, then the last step done
 
-  // pinned host mirror of the current PDF array
+  // pinned host mirror of the current PDF array (FP64 whatever the storage)
   double* mirror;
   size_t mirrorElems;
   bool dirty;
+  int storage;       // lbm::kStoreF64 / F32 / F16
+  size_t elemBytes;  // bytes per stored PDF
+  void* rawStage;    // pinned staging buffer of the device format (reduced storage)
 
   // device memory
   double* dF;
@@ -82,12 +85,14 @@ struct Gpu {
 void usage() {
   std::printf("Kernel parameters:\n");
   std::printf("  [-lambda <v|a/b>] [-blk <n>] [-blk-[xyz] <n>] [-pad auto|no|m+o(,m+o)*] [-bs <n>]\n");
+  std::printf("  [-precision fp64|fp32|fp16]   (cuda-list-aa-pv-soa: PDF storage; fp32/fp16 relax in FP32)\n");
 }
 
 struct Args {
   double lambda = 1.0 / 12.0;
   int blk[3] = {0, 0, 0};
   const char* pad = nullptr;
+  int storage = lbm::kStoreF64;
 };
 
 Args parse_args(Parameters* p) {
@@ -119,6 +124,15 @@ Args parse_args(Parameters* p) {
       a.blk[axis - 'x'] = v;
     } else if (!std::strcmp(s, "-pad") || !std::strcmp(s, "--pad")) {
       a.pad = need();
+    } else if (!std::strcmp(s, "-precision") || !std::strcmp(s, "--precision")) {
+      const char* v = need();
+      if (!std::strcmp(v, "fp64")) a.storage = lbm::kStoreF64;
+      else if (!std::strcmp(v, "fp32")) a.storage = lbm::kStoreF32;
+      else if (!std::strcmp(v, "fp16")) a.storage = lbm::kStoreF16;
+      else {
+        std::printf("ERROR: -precision must be fp64, fp32 or fp16, got \"%s\".\n", v);
+        std::exit(1);
+      }
     } else if (!std::strcmp(s, "-bs") || !std::strcmp(s, "--bs")) {
       (void)need();  // accepted for command-line compatibility; tiles are fixed per kernel
     } else if (!std::strcmp(s, "-h") || !std::strcmp(s, "-help") || !std::strcmp(s, "--help")) {
@@ -151,6 +165,26 @@ lbm::Trt<double> make_trt(double omega, double lambda, double xforce) {
   for (int d = 0; d < Q; ++d) t.force[d] = 3.0 * w[d] * lbm::cx(d) * xforce;
   return t;
 }
+
+lbm::Trt<float> to_float(const lbm::Trt<double>& d) {
+  lbm::Trt<float> t;
+  t.omegaEven = (float)d.omegaEven;
+  t.omegaOdd = (float)d.omegaOdd;
+  t.w0 = (float)d.w0;
+  t.w1 = (float)d.w1;
+  t.w2 = (float)d.w2;
+  t.w1x3 = (float)d.w1x3;
+  t.w2x3 = (float)d.w2x3;
+  t.w1nh = (float)d.w1nh;
+  t.w2nh = (float)d.w2nh;
+  for (int k = 0; k < Q; ++k) t.force[k] = (float)d.force[k];
+  return t;
+}
+
+// Weights and FP16 scales per direction (the device's StoreF16 uses the same
+// powers of two).
+double weight_of(int d) { return d == lbm::DC ? 1.0 / 3.0 : (lbm::cx(d) * lbm::cx(d) + lbm::cy(d) * lbm::cy(d) + lbm::cz(d) * lbm::cz(d) == 1 ? 1.0 / 18.0 : 1.0 / 36.0); }
+double f16_scale_of(int d) { return d == lbm::DC ? 32768.0 : (weight_of(d) > 0.05 ? 262144.0 : 524288.0); }
 
 // --- logical node view on the mirror ---------------------------------------
 
@@ -232,6 +266,16 @@ lbm::ListArgs list_args(Gpu* g) {
   return a;
 }
 
+lbm::ListArgsLp list_args_lp(Gpu* g) {
+  lbm::ListArgsLp a;
+  a.f = g->dF;
+  a.adj = g->dAdj;
+  a.nCells = g->nCells;
+  a.nFluid = g->nFluid;
+  a.err = g->dErr;
+  return a;
+}
+
 double* current_grid(Gpu* g) { return (g->kind == kListPull && g->cur == 1) ? g->dG : g->dF; }
 
 // Enqueues n time steps (AA kernels: rounded up to whole even/odd pairs, as
@@ -245,12 +289,30 @@ long enqueue_steps(Gpu* g, const lbm::Trt<double>& t, int n, cudaEvent_t* ev = n
   };
   if (g->kind == kAa) {
     lbm::AaArgs a = aa_args(g);
+    const bool interior = lbm::aa_has_interior(a);
     for (int it = 0; it < n; it += 2) {
       mark();
       lbm::aa_even_fp64(a, t, g->stream);
       ++k;
+      if (interior) {
+        mark();
+        lbm::aa_odd_interior_fp64(a, t, g->stream);
+        ++k;
+      }
       mark();
-      lbm::aa_odd_fp64(a, t, g->stream);
+      lbm::aa_odd_face_fp64(a, t, g->stream);
+      ++k;
+      g->iteration = it + 1;
+    }
+  } else if (g->kind == kListAa && g->storage != lbm::kStoreF64) {
+    const lbm::ListArgsLp a = list_args_lp(g);
+    const lbm::Trt<float> tf = to_float(t);
+    for (int it = 0; it < n; it += 2) {
+      mark();
+      lbm::list_even_lp(a, tf, g->storage, g->stream);
+      ++k;
+      mark();
+      lbm::list_odd_lp(a, tf, g->storage, g->stream);
       ++k;
       g->iteration = it + 1;
     }
@@ -279,22 +341,62 @@ long enqueue_steps(Gpu* g, const lbm::Trt<double>& t, int n, cudaEvent_t* ev = n
   return k;
 }
 
-long launches_for(const Gpu* g, int n) { return g->kind == kListPull ? n : 2L * ((n + 1) / 2); }
+long launches_for(Gpu* g, int n) {
+  if (g->kind == kListPull) return n;
+  const long perPair = g->kind == kAa ? (lbm::aa_has_interior(aa_args(g)) ? 3 : 2) : 2;
+  return perPair * ((n + 1) / 2);
+}
+
+// Host-side conversion between the FP64 mirror and the device storage format
+// (element k belongs to direction k / nCells).
+void mirror_to_raw(Gpu* g) {
+  const size_t n = g->mirrorElems, nc = (size_t)g->nCells;
+  if (g->storage == lbm::kStoreF32) {
+    float* r = static_cast<float*>(g->rawStage);
+    for (size_t k = 0; k < n; ++k) r[k] = (float)g->mirror[k];
+  } else {
+    uint16_t* r = static_cast<uint16_t*>(g->rawStage);
+    for (size_t k = 0; k < n; ++k) {
+      const int d = (int)(k / nc);
+      r[k] = lbmh_f32_to_f16((float)((g->mirror[k] - weight_of(d)) * f16_scale_of(d)));
+    }
+  }
+}
+
+void raw_to_mirror(Gpu* g) {
+  const size_t n = g->mirrorElems, nc = (size_t)g->nCells;
+  if (g->storage == lbm::kStoreF32) {
+    const float* r = static_cast<const float*>(g->rawStage);
+    for (size_t k = 0; k < n; ++k) g->mirror[k] = (double)r[k];
+  } else {
+    const uint16_t* r = static_cast<const uint16_t*>(g->rawStage);
+    for (size_t k = 0; k < n; ++k) {
+      const int d = (int)(k / nc);
+      g->mirror[k] = weight_of(d) + (double)lbmh_f16_to_f32(r[k]) / f16_scale_of(d);
+    }
+  }
+}
 
 void upload_if_dirty(Gpu* g) {
   g->lastH2D = 0;
   if (!g->dirty) return;
-  LBM_CK(cudaMemcpyAsync(current_grid(g), g->mirror, g->mirrorElems * sizeof(double), cudaMemcpyHostToDevice,
-                         g->stream));
-  g->lastH2D = g->mirrorElems * sizeof(double);
+  const void* src = g->mirror;
+  if (g->storage != lbm::kStoreF64) {
+    LBM_CK(cudaStreamSynchronize(g->stream));
+    mirror_to_raw(g);
+    src = g->rawStage;
+  }
+  LBM_CK(cudaMemcpyAsync(current_grid(g), src, g->mirrorElems * g->elemBytes, cudaMemcpyHostToDevice, g->stream));
+  g->lastH2D = g->mirrorElems * g->elemBytes;
   g->dirty = false;
 }
 
 void download(Gpu* g) {
-  LBM_CK(cudaMemcpyAsync(g->mirror, current_grid(g), g->mirrorElems * sizeof(double), cudaMemcpyDeviceToHost,
-                         g->stream));
+  void* dst = g->storage == lbm::kStoreF64 ? static_cast<void*>(g->mirror) : g->rawStage;
+  LBM_CK(cudaMemcpyAsync(dst, current_grid(g), g->mirrorElems * g->elemBytes, cudaMemcpyDeviceToHost, g->stream));
   LBM_CK(cudaStreamSynchronize(g->stream));
-  g->lastD2H = g->mirrorElems * sizeof(double);
+  if (g->storage != lbm::kStoreF64) raw_to_mirror(g);
+  g->lastD2H = g->mirrorElems * g->elemBytes;
 }
 
 void check_device_error(Gpu* g) {
@@ -341,6 +443,12 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params) {
   Args a = parse_args(params);
   g->kind = kind;
   g->lambda = a.lambda;
+  g->storage = a.storage;
+  g->elemBytes = a.storage == lbm::kStoreF64 ? 8 : (a.storage == lbm::kStoreF32 ? 4 : 2);
+  if (a.storage != lbm::kStoreF64 && kind != kListAa) {
+    std::printf("ERROR: -precision fp32/fp16 is available for cuda-list-aa-pv-soa only.\n");
+    std::exit(1);
+  }
   g->iteration = -1;
   for (int i = 0; i < 3; ++i) g->dims[i] = ld->Dims[i];
   g->per[0] = ld->PeriodicX;
@@ -406,8 +514,8 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params) {
     LBM_CK(cudaMalloc(&g->dAdj, sizeof(uint32_t) * adjElems));
     LBM_CK(cudaMemcpy(g->dAdj, g->adjHost, sizeof(uint32_t) * adjElems, cudaMemcpyHostToDevice));
     g->mirrorElems = (size_t)Q * nCells;
-    LBM_CK(cudaMalloc(&g->dF, sizeof(double) * g->mirrorElems));
-    LBM_CK(cudaMemset(g->dF, 0, sizeof(double) * g->mirrorElems));
+    LBM_CK(cudaMalloc(&g->dF, g->elemBytes * g->mirrorElems));
+    LBM_CK(cudaMemset(g->dF, 0, g->elemBytes * g->mirrorElems));
     if (pull) {
       LBM_CK(cudaMalloc(&g->dG, sizeof(double) * g->mirrorElems));
       LBM_CK(cudaMemset(g->dG, 0, sizeof(double) * g->mirrorElems));
@@ -416,12 +524,19 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params) {
     kd->GlobalDims[1] = ld->Dims[1];
     kd->GlobalDims[2] = ld->Dims[2];
     // the GPU odd step reads all 18 adjacency entries of a node every time
-    kd->LoopBalance = pull ? 2.0 * 19 * 8 + 18 * 4.0 : (2.0 * 19 * 8 + (2.0 * 19 * 8 + 18 * 4.0)) / 2.0;
+    const double pb = 2.0 * 19 * (double)g->elemBytes;
+    kd->LoopBalance = pull ? pb + 18 * 4.0 : (pb + (pb + 18 * 4.0)) / 2.0;
   }
 
   LBM_CK(cudaMallocHost(&g->mirror, sizeof(double) * g->mirrorElems));
   std::memset(g->mirror, 0, sizeof(double) * g->mirrorElems);
   g->dirty = false;  // device and mirror both hold zeros
+  if (g->storage != lbm::kStoreF64) {
+    LBM_CK(cudaMallocHost(&g->rawStage, g->elemBytes * g->mirrorElems));
+    // the device holds raw zeros; keep the mirror consistent with them
+    LBM_CK(cudaMemcpy(g->rawStage, g->dF, g->elemBytes * g->mirrorElems, cudaMemcpyDeviceToHost));
+    raw_to_mirror(g);
+  }
   kd->Pdfs[0] = g->mirror;
   kd->Pdfs[1] = nullptr;
   kd->PdfsActive = g->mirror;
@@ -438,6 +553,7 @@ void gpu_free(KernelData** kernelData) {
   cudaFree(g->dAdj);
   cudaFree(g->dErr);
   cudaFreeHost(g->mirror);
+  cudaFreeHost(g->rawStage);
   cudaEventDestroy(g->ev0);
   cudaEventDestroy(g->ev1);
   cudaStreamDestroy(g->stream);
@@ -551,6 +667,16 @@ int lbm_b200_time_steps(KernelData* kd, CaseData* cd, int n, double* total_ms, d
   int err = 0;
   cudaMemcpy(&err, g->dErr, sizeof(int), cudaMemcpyDeviceToHost);
   if (err) { g_lastError = "a device wait exceeded its limit"; return -1; }
+  return 0;
+}
+
+int lbm_b200_device_state(KernelData* kd, double** pdfs, long long* nCells, int* nFluid, void** stream) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (g->kind == kAa) return -1;
+  if (pdfs) *pdfs = current_grid(g);
+  if (nCells) *nCells = g->nCells;
+  if (nFluid) *nFluid = g->nFluid;
+  if (stream) *stream = g->stream;
   return 0;
 }
 

@@ -84,4 +84,31 @@ __device__ __forceinline__ void trt_collide(const Trt<R>& t, const R* f, R* out)
   trt_pair(t, f, out, TN, BS, uy + uz, t.w2nh, t.w2x3, w2i);
 }
 
+// An opaque copy of a pointer: the compiler cannot tell that it equals its
+// source, so addresses formed from it are not shared with (and do not keep
+// alive) addresses formed from the original. Used to give the store phase its
+// own addresses, which frees the load addresses' registers across the
+// collision.
+template <typename P>
+__device__ __forceinline__ P* launder(P* p) {
+  P* q;
+  asm volatile("mov.b64 %0, %1;" : "=l"(q) : "l"(p));
+  return q;
+}
+
+// One node update through accessors: all 19 loads are issued first (they are
+// independent, so they are in flight together), then the relaxation, then
+// the 19 stores. `load(d)` returns the incoming PDF of direction d,
+// `store(d, v)` writes the post-collision PDF of direction d to its
+// destination.
+template <typename R, class Load, class Store>
+__device__ __forceinline__ void trt_update(const Trt<R>& t, Load load, Store store) {
+  R f[Q], o[Q];
+#pragma unroll
+  for (int d = 0; d < Q; ++d) f[d] = load(d);
+  trt_collide(t, f, o);
+#pragma unroll
+  for (int d = 0; d < Q; ++d) store(d, o[d]);
+}
+
 }  // namespace lbm

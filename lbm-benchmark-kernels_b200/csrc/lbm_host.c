@@ -611,3 +611,55 @@ int lbm_geo_spheres(const int dims[3], uint64_t seed, double porosity, double rm
 	free(sp); free(next); free(head);
 	return 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* IEEE 754 binary16 conversions for the FP16 mirror (round to nearest even),
+ * written from the format definition: 1 sign bit, 5 exponent bits (bias 15),
+ * 10 fraction bits; subnormals below 2^-14. */
+
+float lbmh_f16_to_f32(uint16_t h)
+{
+	const uint32_t sign = (uint32_t)(h & 0x8000u) << 16;
+	const uint32_t ex = (h >> 10) & 0x1fu, fr = h & 0x3ffu;
+	uint32_t bits;
+	if (ex == 0) {
+		if (fr == 0) bits = sign;
+		else {
+			/* subnormal: value = fr * 2^-24 */
+			float v = (float)fr * 5.9604644775390625e-08f;
+			memcpy(&bits, &v, 4);
+			bits |= sign;
+		}
+	}
+	else if (ex == 31) bits = sign | 0x7f800000u | (fr << 13);
+	else bits = sign | ((ex + 112u) << 23) | (fr << 13);
+	float out;
+	memcpy(&out, &bits, 4);
+	return out;
+}
+
+uint16_t lbmh_f32_to_f16(float f)
+{
+	uint32_t x;
+	memcpy(&x, &f, 4);
+	const uint16_t sign = (uint16_t)((x >> 16) & 0x8000u);
+	const uint32_t ax = x & 0x7fffffffu;
+	if (ax >= 0x7f800000u) return sign | (ax > 0x7f800000u ? 0x7e00u : 0x7c00u); /* NaN / inf */
+	if (ax >= 0x477ff000u) return sign | 0x7c00u;                               /* rounds above 65504 */
+	if (ax < 0x38800000u) {
+		/* result subnormal or zero: round fr * 2^-24 to an integer, ties to even */
+		float v;
+		memcpy(&v, &ax, 4);
+		float q = v * 16777216.0f; /* exact scaling by 2^24 */
+		uint32_t i = (uint32_t)q;
+		float rem = q - (float)i;
+		if (rem > 0.5f || (rem == 0.5f && (i & 1u))) ++i;
+		return sign | (uint16_t)i;
+	}
+	/* normal: drop 13 fraction bits with round to nearest even */
+	uint32_t m = ax + 0xc8000000u; /* rebias exponent 127 -> 15 (subtract 112 << 23) */
+	uint32_t r = m >> 13;
+	uint32_t rest = m & 0x1fffu;
+	if (rest > 0x1000u || (rest == 0x1000u && (r & 1u))) ++r;
+	return sign | (uint16_t)r;
+}

@@ -39,6 +39,10 @@ int lbmh_list_build(const LatticeDesc *ld, int pull, const int blk[3], int nCell
  * get 0. cellOf(x,y,z) = (x+1)*xs + (y+1)*pitch + z + zoff. */
 void lbmh_aa_links(const LatticeDesc *ld, int xs, int pitch, int zoff, uint32_t *link);
 
+/* IEEE binary16 <-> binary32 (round to nearest even). */
+float lbmh_f16_to_f32(uint16_t h);
+uint16_t lbmh_f32_to_f16(float f);
+
 /* Parses "v" or "a/b" into a double; returns 0 on success. */
 int lbmh_parse_fraction(const char *s, double *out);
 

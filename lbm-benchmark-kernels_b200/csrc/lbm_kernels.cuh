@@ -55,11 +55,38 @@ struct ListArgs {
   int* err;       // device error word (bounded waits)
 };
 
+// Reduced-storage list AA (lbm_kernels_lp.cu): PDFs stored as FP32 or as
+// scaled FP16 deviations from the weights, collision in FP32.
+constexpr int kStoreF64 = 0;
+constexpr int kStoreF32 = 1;
+constexpr int kStoreF16 = 2;
+
+struct ListArgsLp {
+  void* f;  // float or __half, f[d * nCells + n]
+  const uint32_t* adj;
+  long long nCells;
+  int nFluid;
+  int* err;
+};
+
 // Launchers (stream-ordered, no synchronisation).
+void list_even_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s);
+void list_odd_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s);
 void aa_even_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
-void aa_odd_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
+// The AA odd step is two launches: the interior cells, then the face shell.
+void aa_odd_interior_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
+void aa_odd_face_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
+bool aa_has_interior(const AaArgs& a);
+long long aa_shell_cells(const AaArgs& a);
 void list_even_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
 void list_odd_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
 void list_pull_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
+
+// FP64 mass and momentum sums of a list-layout field (lbm_moments.cu):
+// pass 1 writes 4 partial sums per block of kListTile nodes into `partials`
+// (moment_blocks(nFluid) * 4 doubles), pass 2 folds them into out[0..3] =
+// {sum rho, sum j_x, sum j_y, sum j_z}.
+int moment_blocks(int nFluid);
+void moments_enqueue(const double* f, long long nCells, int nFluid, double* partials, double* out, cudaStream_t s);
 
 }  // namespace lbm

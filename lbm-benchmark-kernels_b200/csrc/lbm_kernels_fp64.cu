@@ -66,64 +66,129 @@ __global__ void __launch_bounds__(128) k_aa_even_fp64(const AaArgs a, const Trt<
   if (z >= a.nZ || y >= a.nY) return;
   const int c = aa_cell(a, x, y, z);
   if (!(__ldg(a.link + c) & kFluidBit)) return;
-
-  double f[Q], o[Q];
-#pragma unroll
-  for (int d = 0; d < Q; ++d) f[d] = a.f[d * a.dstride + c];
-  trt_collide(t, f, o);
-#pragma unroll
-  for (int d = 0; d < Q; ++d) a.f[inv(d) * a.dstride + c] = o[d];
+  double* const f = a.f + c;
+  double* const fs = launder(f);
+  const long long S = a.dstride;
+  // local collide; the post-collision PDF of direction d goes to slot inv(d)
+  trt_update(t, [&](int d) { return f[d * S]; }, [&](int d, double v) { fs[inv(d) * S] = v; });
 }
 
-__global__ void __launch_bounds__(128) k_aa_odd_fp64(const AaArgs a, const Trt<double> t) {
-  const int z = blockIdx.x * 32 + threadIdx.x;
-  const int y = blockIdx.y * 4 + threadIdx.y;
-  const int x = blockIdx.z;
-  if (z >= a.nZ || y >= a.nY) return;
+// Odd step. Node x reads its incoming f_i from slot (x + c_j, j), j = inv(i)
+// (the AA pattern: the slots a node reads are the slots it writes), plus the
+// body-force increment of that post-even logical PDF; it writes f_i to slot
+// (x + c_i, i) with the increment of i, or -- bounced back at a wall -- to
+// its own slot (x, inv(i)) with the increment of inv(i).
+//
+// Two kernels share the step. The interior kernel takes the cells off every
+// domain face: no link of theirs can leave the domain, so each address is a
+// select between the neighbour's slot and the node's own slot, and the 19
+// loads are issued together. The face kernel takes the one-cell shell: links
+// that leave the domain wrap periodically on every crossed axis, or, at a
+// non-periodic face, go to the ghost layer (an "open" link), as in the
+// reference.
+__global__ void __launch_bounds__(128) k_aa_odd_interior_fp64(const AaArgs a, const Trt<double> t) {
+  const int z = 1 + blockIdx.x * 32 + threadIdx.x;
+  const int y = 1 + blockIdx.y * 4 + threadIdx.y;
+  const int x = 1 + blockIdx.z;
+  if (z > a.nZ - 2 || y > a.nY - 2) return;
   const int c = aa_cell(a, x, y, z);
   const uint32_t w = __ldg(a.link + c);
   if (!(w & kFluidBit)) return;
-  const bool edge = x == 0 || y == 0 || z == 0 || x == a.nX - 1 || y == a.nY - 1 || z == a.nZ - 1;
-
-  double f[Q], o[Q];
-  // Incoming PDF of direction i comes from x - c_i = x + c_inv(i).
-#pragma unroll
-  for (int i = 0; i < QM; ++i) {
-    const int j = inv(i);
-    double v;
-    if ((w >> j) & 1u) {
-      if (edge && aa_open(a, x, y, z, j))
-        v = a.f[j * a.dstride + c + aa_off(a, j)];  // ghost slot, as the reference
-      else
-        v = a.f[i * a.dstride + c];  // bounce back: own slot of direction i
-    } else {
-      const int nc = edge ? aa_wrapped(a, x, y, z, j) : c + aa_off(a, j);
-      v = a.f[j * a.dstride + nc];
+  const long long S = a.dstride;
+  double* const f = a.f;
+  double* const fs = launder(f);
+  auto load = [&](int d) -> double {
+    if (d == DC) return f[DC * S + c] + t.force[DC];
+    const int j = inv(d);
+    const bool rev = (w >> j) & 1u;
+    return f[rev ? d * S + c : j * S + c + aa_off(a, j)] + t.force[d];
+  };
+  auto store = [&](int d, double v) {
+    if (d == DC) {
+      fs[DC * S + c] = v + t.force[DC];
+      return;
     }
-    f[i] = v + t.force[i];
-  }
-  f[DC] = a.f[DC * a.dstride + c] + t.force[DC];
-
-  trt_collide(t, f, o);
-
-#pragma unroll
-  for (int i = 0; i < QM; ++i) {
-    const int j = inv(i);
-    if ((w >> i) & 1u) {
-      if (edge && aa_open(a, x, y, z, i)) {
-        a.f[i * a.dstride + c + aa_off(a, i)] = o[i];
-        double* own = a.f + j * a.dstride + c;
-        *own = *own + t.force[j];
-      } else {
-        a.f[j * a.dstride + c] = o[i] + t.force[j];
-      }
-    } else {
-      const int nc = edge ? aa_wrapped(a, x, y, z, i) : c + aa_off(a, i);
-      a.f[i * a.dstride + nc] = o[i] + t.force[i];
-    }
-  }
-  a.f[DC * a.dstride + c] = o[DC] + t.force[DC];
+    const int j = inv(d);
+    const bool rev = (w >> d) & 1u;
+    fs[rev ? j * S + c : d * S + c + aa_off(a, d)] = v + (rev ? t.force[j] : t.force[d]);
+  };
+  trt_update(t, load, store);
 }
+
+// Cell of shell index i: the x faces (all y, z), then the y faces (inner x,
+// all z), then the z faces (inner x and y). A one-cell-thin axis has a single
+// face.
+__device__ __forceinline__ void aa_shell_cell(const AaArgs& a, long long i, int& x, int& y, int& z) {
+  const long long nY = a.nY, nZ = a.nZ;
+  const long long sx = a.nX > 1 ? 2 : 1, sy = a.nY > 1 ? 2 : 1;
+  const long long mx = a.nX > 2 ? a.nX - 2 : 0, my = a.nY > 2 ? a.nY - 2 : 0;
+  const long long nA = sx * nY * nZ, nB = sy * mx * nZ;
+  if (i < nA) {
+    x = (i / (nY * nZ)) == 0 ? 0 : a.nX - 1;
+    const long long r = i % (nY * nZ);
+    y = (int)(r / nZ);
+    z = (int)(r % nZ);
+  } else if (i < nA + nB) {
+    const long long j = i - nA;
+    y = (j / (mx * nZ)) == 0 ? 0 : a.nY - 1;
+    const long long r = j % (mx * nZ);
+    x = 1 + (int)(r / nZ);
+    z = (int)(r % nZ);
+  } else {
+    const long long k = i - nA - nB;
+    z = (k / (mx * my)) == 0 ? 0 : a.nZ - 1;
+    const long long r = k % (mx * my);
+    x = 1 + (int)(r / my);
+    y = 1 + (int)(r % my);
+  }
+}
+
+__global__ void __launch_bounds__(128) k_aa_odd_face_fp64(const AaArgs a, const Trt<double> t, long long nShell) {
+  const long long i = static_cast<long long>(blockIdx.x) * 128 + threadIdx.x;
+  if (i >= nShell) return;
+  int x, y, z;
+  aa_shell_cell(a, i, x, y, z);
+  const int c = aa_cell(a, x, y, z);
+  const uint32_t w = __ldg(a.link + c);
+  if (!(w & kFluidBit)) return;
+  const long long S = a.dstride;
+  double* const f = a.f;
+  auto load = [&](int d) -> double {
+    if (d == DC) return f[DC * S + c] + t.force[DC];
+    const int j = inv(d);
+    const bool rev = (w >> j) & 1u;
+    const bool open = rev && aa_open(a, x, y, z, j);
+    const int nb = rev ? c + aa_off(a, j) : aa_wrapped(a, x, y, z, j);
+    return f[(rev && !open) ? d * S + c : j * S + nb] + t.force[d];
+  };
+  auto store = [&](int d, double v) {
+    if (d == DC) {
+      f[DC * S + c] = v + t.force[DC];
+      return;
+    }
+    const int j = inv(d);
+    const bool rev = (w >> d) & 1u;
+    if (!rev) {
+      f[d * S + aa_wrapped(a, x, y, z, d)] = v + t.force[d];
+    } else if (aa_open(a, x, y, z, d)) {
+      // open face: the PDF leaves into the ghost layer; the node's own slot
+      // of direction inv(d) keeps its even-step value and gets its increment
+      f[d * S + c + aa_off(a, d)] = v;
+      f[j * S + c] = f[j * S + c] + t.force[j];
+    } else {
+      f[j * S + c] = v + t.force[j];
+    }
+  };
+  trt_update(t, load, store);
+}
+
+long long aa_shell_cells(const AaArgs& a) {
+  const long long sx = a.nX > 1 ? 2 : 1, sy = a.nY > 1 ? 2 : 1, sz = a.nZ > 1 ? 2 : 1;
+  const long long mx = a.nX > 2 ? a.nX - 2 : 0, my = a.nY > 2 ? a.nY - 2 : 0;
+  return sx * a.nY * a.nZ + sy * mx * a.nZ + sz * mx * my;
+}
+
+bool aa_has_interior(const AaArgs& a) { return a.nX > 2 && a.nY > 2 && a.nZ > 2; }
 
 static dim3 aa_grid(const AaArgs& a) { return dim3((a.nZ + 31) / 32, (a.nY + 3) / 4, a.nX); }
 
@@ -131,22 +196,27 @@ void aa_even_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
   k_aa_even_fp64<<<aa_grid(a), dim3(32, 4), 0, s>>>(a, t);
 }
 
-void aa_odd_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
-  k_aa_odd_fp64<<<aa_grid(a), dim3(32, 4), 0, s>>>(a, t);
+void aa_odd_interior_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
+  if (!aa_has_interior(a)) return;
+  k_aa_odd_interior_fp64<<<dim3((a.nZ - 2 + 31) / 32, (a.nY - 2 + 3) / 4, a.nX - 2), dim3(32, 4), 0, s>>>(a, t);
+}
+
+void aa_odd_face_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
+  const long long n = aa_shell_cells(a);
+  k_aa_odd_face_fp64<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a, t, n);
 }
 
 // ---------------------------------------------------------------------------
 // Fluid-node lists.
 
-__global__ void __launch_bounds__(kListTile) k_list_even_fp64(const ListArgs a, const Trt<double> t) {
+// 4 blocks of 256 threads per SM (64 registers, no spills)
+__global__ void __launch_bounds__(kListTile, 4) k_list_even_fp64(const ListArgs a, const Trt<double> t) {
   const int n = blockIdx.x * kListTile + threadIdx.x;
   if (n >= a.nFluid) return;
-  double f[Q], o[Q];
-#pragma unroll
-  for (int d = 0; d < Q; ++d) f[d] = a.f[d * a.nCells + n];
-  trt_collide(t, f, o);
-#pragma unroll
-  for (int d = 0; d < Q; ++d) a.f[inv(d) * a.nCells + n] = o[d];
+  double* const f = a.f + n;
+  double* const fs = launder(f);
+  const long long S = a.nCells;
+  trt_update(t, [&](int d) { return f[d * S]; }, [&](int d, double v) { fs[inv(d) * S] = v; });
 }
 
 // Stages the block's adjacency tile (kListTile nodes x 18 entries, contiguous)
@@ -166,44 +236,33 @@ __device__ __forceinline__ bool stage_adj_tile(const ListArgs& a, uint32_t* sadj
   return true;
 }
 
-// Reads the 18 entries of node `t` of the tile as 9 8-byte words (conflict
-// free: 18 words apart per thread).
-__device__ __forceinline__ void load_adj(const uint32_t* sadj, int t, uint32_t* e) {
-  const uint2* p = reinterpret_cast<const uint2*>(sadj + t * QM);
-#pragma unroll
-  for (int k = 0; k < QM / 2; ++k) {
-    uint2 v = p[k];
-    e[2 * k] = v.x;
-    e[2 * k + 1] = v.y;
-  }
-}
-
-__global__ void __launch_bounds__(kListTile) k_list_odd_fp64(const ListArgs a, const Trt<double> t) {
+// 3 blocks of 256 threads per SM (80 registers, no spills)
+__global__ void __launch_bounds__(kListTile, 3) k_list_odd_fp64(const ListArgs a, const Trt<double> t) {
   __shared__ alignas(128) uint32_t sadj[kListTile * QM];
   __shared__ alignas(8) uint64_t bar;
   if (!stage_adj_tile(a, sadj, &bar)) return;
   const int n = blockIdx.x * kListTile + threadIdx.x;
   if (n >= a.nFluid) return;
+  const uint32_t* e = sadj + threadIdx.x * QM;  // this node's 18 links
+  double* const f = a.f;
+  const long long S = a.nCells;
 
-  uint32_t e[QM];
-  load_adj(sadj, threadIdx.x, e);
-
-  double f[Q], o[Q];
-#pragma unroll
-  for (int i = 0; i < QM; ++i) f[i] = a.f[e[inv(i)]] + t.force[i];
-  f[DC] = a.f[DC * a.nCells + n] + t.force[DC];
-
-  trt_collide(t, f, o);
-
-#pragma unroll
-  for (int i = 0; i < QM; ++i) {
-    const int j = inv(i);
-    // A link that points back to the node itself is a bounce back: the PDF
-    // becomes direction inv(i) of this node.
-    const bool bounce = e[i] == static_cast<uint32_t>(j * a.nCells + n);
-    a.f[e[i]] = o[i] + (bounce ? t.force[j] : t.force[i]);
-  }
-  a.f[DC * a.nCells + n] = o[DC] + t.force[DC];
+  // incoming f_d (the post-even logical PDF) through link inv(d), plus its
+  // body-force increment
+  auto load = [&](int d) -> double {
+    return (d == DC ? f[DC * S + n] : f[e[inv(d)]]) + t.force[d];
+  };
+  // outgoing f_d through link d; a link that points back to the node itself
+  // is a bounce back: the PDF becomes direction inv(d) of this node and gets
+  // the increment of inv(d)
+  auto store = [&](int d, double v) {
+    if (d == DC) { f[DC * S + n] = v + t.force[DC]; return; }
+    const uint32_t dst = reinterpret_cast<const volatile uint32_t*>(e)[d];  // re-read: keeps no 64-bit addresses live across the collision
+    const int j = inv(d);
+    const bool bounce = dst == static_cast<uint32_t>(j * S + n);
+    f[dst] = v + (bounce ? t.force[j] : t.force[d]);
+  };
+  trt_update(t, load, store);
 }
 
 __global__ void __launch_bounds__(kListTile) k_list_pull_fp64(const ListArgs a, const Trt<double> t) {
@@ -212,17 +271,17 @@ __global__ void __launch_bounds__(kListTile) k_list_pull_fp64(const ListArgs a, 
   if (!stage_adj_tile(a, sadj, &bar)) return;
   const int n = blockIdx.x * kListTile + threadIdx.x;
   if (n >= a.nFluid) return;
-
-  uint32_t e[QM];
-  load_adj(sadj, threadIdx.x, e);
-
+  const uint32_t* e = sadj + threadIdx.x * QM;
+  const long long S = a.nCells;
+  // one pass: the gathers are issued together and the 19 outputs are
+  // contiguous stores to the second grid
   double f[Q], o[Q];
-  f[DC] = a.f[DC * a.nCells + n];
+  f[DC] = a.f[DC * S + n];
 #pragma unroll
   for (int d = 0; d < QM; ++d) f[d] = a.f[e[d]];
   trt_collide(t, f, o);
 #pragma unroll
-  for (int d = 0; d < Q; ++d) a.g[d * a.nCells + n] = o[d] + t.force[d];
+  for (int d = 0; d < Q; ++d) a.g[d * S + n] = o[d] + t.force[d];
 }
 
 static unsigned list_blocks(const ListArgs& a) { return (a.nFluid + kListTile - 1) / kListTile; }
