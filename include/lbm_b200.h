@@ -235,6 +235,19 @@ void lbm_b200_set_field(KernelData *kd, LatticeDesc *ld, const double *in);
  * Returns -1 for the full-array kernel. */
 int lbm_b200_list_layout(KernelData *kd, const uint32_t **grid, const uint32_t **adj, int *nFluid, int *nCells);
 
+/* The same sums for callers that cannot allocate device memory: code that
+ * runs while another component owns the device allocator, or that may only
+ * use the buffers its host application hands it. Has no counterpart in the
+ * reference. The reduction's scratch is a fixed 2 MiB array inside the
+ * library (held by every GPU that loads it until the process exits), so a call
+ * accepts at most 16,777,216 fluid nodes and returns -2 (with a message) above
+ * that. Allocates nothing; does not synchronise (the result is ready when the
+ * stream is). The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and should come before any stream capture. Calls
+ * share the array: calls that overlap on the GPU race. Returns 0, -1 for bad
+ * arguments, or a CUDA error code. */
+int lbm_b200_moments_noalloc(const double *pdfs, long long nCells, int nFluid, double *out_device, void *stream);
+
 /* Host layout builders (no GPU needed), exported for the parity tests:
  * SoA padding (src/Padding.c:195-244), list numbering + adjacency
  * (src/BenchKernelD3Q19ListAaPvCommon.c:587-792; pull variant
