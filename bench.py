@@ -54,49 +54,10 @@ def parse():
     p.add_argument("--seed", type=int, default=20251203)
     p.add_argument("--no-extra", action="store_true", help="skip the secondary kernel lines")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    p.add_argument("--batched", type=int, default=512, help="domains of the batched form (0 = skip)")
+    p.add_argument("--serving", type=int, default=24, help="requests of the serving form (0 = skip)")
+    p.add_argument("--precision-steps", type=int, default=20000, help="steps of the precision study (0 = skip)")
     return p.parse_args()
-
-
-# ---------------------------------------------------------------------------
-# ranks
-
-class Dist:
-    def __init__(self, n_gpus):
-        self.world = int(os.environ.get("WORLD_SIZE", "1"))
-        self.rank = int(os.environ.get("RANK", "0"))
-        self.local = int(os.environ.get("LOCAL_RANK", "0"))
-        self.pg = None
-        if self.world > 1:
-            import datetime
-
-            import torch
-            import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                    device_id=torch.device("cuda", self.local))
-            self.torch, self.dist = torch, dist
-
-    def barrier(self):
-        if self.world > 1:
-            self.dist.barrier()
-
-    def max(self, v):
-        if self.world == 1:
-            return v
-        t = self.torch.tensor([float(v)], device="cuda")
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum(self, v):
-        if self.world == 1:
-            return v
-        t = self.torch.tensor([float(v)], dtype=self.torch.float64, device="cuda")
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
-        return float(t.item())
-
-    def close(self):
-        if self.world > 1:
-            self.dist.destroy_process_group()
 
 
 # ---------------------------------------------------------------------------
@@ -212,17 +173,18 @@ def time_kernel(lbmb200, kname, lat, steps, warmup, kargs, dist, odd_key):
             rc = L.lbm_b200_time_steps(inst.kdp, ctypes.byref(cd), warmup, ctypes.byref(tot), None)
             if rc:
                 raise RuntimeError(L.lbm_b200_last_error().decode())
-        per_pair = 3 if (kname == "cuda-aa-soa" and min(lat.dims) > 2) else 2
-        n_launch = steps if "pull" in kname else per_pair * ((steps + 1) // 2)
-        per = (ctypes.c_double * n_launch)()
+        pairs = (steps + 1) // 2
+        cap = steps if "pull" in kname else 3 * pairs
+        per = (ctypes.c_double * cap)()
         dist.barrier()
         rc = L.lbm_b200_time_steps(inst.kdp, ctypes.byref(cd), steps, ctypes.byref(tot), per)
         if rc:
             raise RuntimeError(L.lbm_b200_last_error().decode())
         dist.barrier()
-        per = list(per)
+        n_launch = inst.last_launches
+        per = list(per)[:n_launch]
         res = {"ms": tot.value, "launches": n_launch,
-               "steps_run": n_launch if "pull" in kname else 2 * ((steps + 1) // 2),
+               "steps_run": steps if "pull" in kname else 2 * pairs,
                "per_launch_ms": per, "inst": inst}
         return res
     except Exception:
@@ -277,6 +239,116 @@ def cpu_model():
     except OSError:
         pass
     return "unknown"
+
+
+# ---------------------------------------------------------------------------
+# BASELINE configs[3..4] and configs[2]: batched, served, reduced precision
+
+def _batch_domains(n, seed, edge_range=(32, 128), threads=16):
+    """n seeded porous domains: edge U{32..128}, r ~ U[3,8], porosity U[0.3,0.6],
+    omega U[0.8,1.6]; sphere packings generated on host threads (C)."""
+    import concurrent.futures
+
+    import numpy as np
+
+    import lbmb200
+    rng = np.random.default_rng(seed)
+    specs = [(int(rng.integers(edge_range[0], edge_range[1] + 1)), float(rng.uniform(0.3, 0.6)),
+              float(rng.uniform(0.8, 1.6)), seed * 1000 + i) for i in range(n)]
+    with concurrent.futures.ThreadPoolExecutor(threads) as pool:
+        lats = list(pool.map(lambda sp: lbmb200.spheres((sp[0],) * 3, sp[3], sp[1], 3.0, 8.0)[0], specs))
+    return lats, [sp[2] for sp in specs]
+
+
+def section_batched(args, dist, peak):
+    """512 domains in one batch (FP32), autotuned, 100-step CUDA graphs, against
+    the same kernel family run one domain at a time."""
+    import time
+
+    import numpy as np
+
+    import lbmb200
+    L = lbmb200.lib()
+    lats, omegas = _batch_domains(args.batched, 7000 + dist.rank)
+    b = lbmb200.Batch("fp32", budget_gb=150.0, max_domains=args.batched)
+    try:
+        slots = [b.add(l, omega=o, lam=3.0 / 16.0, xforce=1e-5) for l, o in zip(lats, omegas)]
+        if min(slots) < 0:
+            raise RuntimeError("the domains do not fit the HBM budget")
+        nodes = sum(l.n_fluid for l in lats)
+        rows = b.tune(trial_steps=6)
+        cfg = b.launch()
+        b.step(100, graph=True)  # capture and warm the graph
+        b.sync()
+        reps = 3
+        dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            b.step(100, graph=True)
+        b.sync()
+        wall = dist.max(time.perf_counter() - t0)
+        ms_direct = b.time_steps(100)
+        agg = nodes * 100 * reps / wall / 1e6
+        agg_direct = nodes * 100 / (ms_direct / 1e3) / 1e6
+    finally:
+        b.close()
+    # one at a time: a seeded subset of the same domains, each alone with the
+    # single-domain FP32 list kernel (device-timed 100 steps each)
+    sub = list(range(0, len(lats), max(1, len(lats) // 64)))[:64]
+    tot_nodes_steps, tot_s = 0, 0.0
+    for i in sub:
+        lat = lats[i]
+        inst = lbmb200.kernel("cuda-list-aa-pv-soa").init(lat, kernel_args=["-precision", "fp32", "-lambda", "3/16"])
+        try:
+            inst.set_field(np.ascontiguousarray(equilibrium_field(lbmb200, lat)))
+            cd = lbmb200.case(omega=omegas[i], xforce=1e-5, iterations=100)
+            tot = ctypes.c_double(0.0)
+            L.lbm_b200_time_steps(inst.kdp, ctypes.byref(cd), 4, ctypes.byref(tot), None)
+            L.lbm_b200_time_steps(inst.kdp, ctypes.byref(cd), 100, ctypes.byref(tot), None)
+            tot_s += tot.value / 1e3
+            tot_nodes_steps += lat.n_fluid * 100
+        finally:
+            inst.deinit()
+    one = tot_nodes_steps / tot_s / 1e6
+    return {"domains": len(lats), "fluid_nodes": nodes, "storage": "fp32",
+            "mflups_graph": round(dist.sum(agg), 1), "mflups_direct_launch": round(dist.sum(agg_direct), 1),
+            "mflups_one_at_a_time": round(dist.sum(one), 1), "speedup_vs_one_at_a_time": round(agg / one, 2),
+            "one_at_a_time_sample": "%d of %d domains, single-domain FP32 kernel, 100 device-timed steps each"
+                                    % (len(sub), len(lats)),
+            "autotuned": cfg, "tuner_candidates": int(len(rows)),
+            "timing": "wall clock around 3 synchronised replays of a 100-step CUDA graph"}
+
+
+def section_serving(args, dist, peak):
+    """Continuous batching (FP32) against the plain FP64 kernel one request at a
+    time, on the same seeded open-loop stream at 80 % of measured capacity."""
+    from lbmb200 import serving
+    n = args.serving
+    # capacity: the batched server with every request available at t = 0
+    cap_reqs = serving.make_requests(n, rate=0.0, seed=900 + dist.rank)
+    cap_sum, _ = serving.serve_batched(cap_reqs, closed_loop=True, prep_threads=8)
+    rate = 0.8 * cap_sum["solves_per_s"]
+    reqs = serving.make_requests(n, rate=rate, seed=901 + dist.rank)
+    batched, recs = serving.serve_batched(reqs, prep_threads=8)
+    fp64, recs64 = serving.serve_fp64_sequential(reqs)
+    by_id = {r["id"]: r for r in recs64}
+    kerr = max(abs(r["k"] - by_id[r["id"]]["k"]) / abs(by_id[r["id"]]["k"]) for r in recs)
+    return {"requests": n, "arrivals": "Poisson, %.3f/s (0.8 x measured capacity %.3f/s)"
+                                      % (rate, cap_sum["solves_per_s"]),
+            "domain": "edge U{32..192}, porosity U[0.3,0.6], r U[3,8], F_x=1e-5, tol 1e-6 per 100 steps, cap 20000",
+            "batched_fp32": batched, "fp64_one_at_a_time": fp64,
+            "solves_per_s_ratio": round(batched["solves_per_s"] / fp64["solves_per_s"], 3),
+            "max_rel_permeability_diff_fp32_vs_fp64": kerr}
+
+
+def section_precision(args, dist, peak):
+    """The 256^3 packing for N steps in FP64, FP32 and FP16-deviation storage."""
+    import lbmb200
+    from lbmb200 import porous
+    lat, _ = lbmb200.spheres((args.edge,) * 3, args.seed, args.porosity, 6.0, 12.0)
+    res = porous.precision_study(lat, steps=args.precision_steps, xforce=1e-5)
+    res["steps"] = args.precision_steps
+    return res
 
 
 # ---------------------------------------------------------------------------
@@ -417,6 +489,16 @@ def run_ours(args, dist):
                 "odd_ms": round(statistics.mean(tl["per_launch_ms"][1::2]), 5)}
         line["kernels"] = extra
 
+    for name, fn, enabled in (("batched", section_batched, args.batched > 0),
+                              ("serving", section_serving, args.serving > 0),
+                              ("precision", section_precision, args.precision_steps > 0 and dist.world == 1)):
+        if not enabled:
+            continue
+        try:
+            line[name] = fn(args, dist, peak)
+        except Exception as e:  # a failing extra must not lose the headline line
+            line[name] = {"error": "%s: %s" % (type(e).__name__, e)}
+
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
         probe = cpu_reference(lat, 2)
         if probe is not None:
@@ -434,7 +516,8 @@ def run_ours(args, dist):
 
 def main():
     args = parse()
-    dist = Dist(args.gpus)
+    from lbmb200.ranks import Ranks
+    dist = Ranks(timeout_s=120)
     try:
         if args.impl == "reference":
             return run_reference_arm(args, dist)

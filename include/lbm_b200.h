@@ -204,6 +204,14 @@ void lbm_b200_mark_mirror_dirty(KernelData *kd);
  * error code. */
 int lbm_b200_time_steps(KernelData *kd, CaseData *cd, int n, double *total_ms, double *per_launch_ms);
 
+/* Runs a kernel that waits, with a bound of `polls` reads, on a device flag
+ * that nothing sets: the wait runs out, the kernel records error bit 2 in its
+ * error word and returns, and *status receives the word (2). The same bounded
+ * pattern guards every device wait of the library (the adjacency bulk copies),
+ * whose error word the host checks after each Kernel call. Returns 0 or a
+ * CUDA error code. */
+int lbm_b200_selftest_bounded_wait(unsigned polls, int *status);
+
 /* Selects the CUDA device used by subsequent Init calls of this thread. */
 int lbm_b200_set_device(int device);
 
@@ -220,6 +228,11 @@ int lbm_b200_device_state(KernelData *kd, double **pdfs, long long *nCells, int 
  * scratch of 4 doubles per 256 nodes with cudaMalloc; stream may be NULL.
  * Synchronises the stream. Returns 0, or a CUDA error code / -1. */
 int lbm_b200_moments_device(const double *pdfs, long long nCells, int nFluid, double *out_device, void *stream);
+
+/* The same sums for an FP64 list-kernel instance, into host memory
+ * (out[0..3]); waits for the instance's pending steps. Returns 0, -1 for the
+ * full-array kernel or reduced storage, or a CUDA error code. */
+int lbm_b200_instance_moments(KernelData *kd, double *out);
 
 /* Last CUDA error string seen by the library ("" if none). */
 const char *lbm_b200_last_error(void);
@@ -255,6 +268,43 @@ int lbm_b200_moments_noalloc(const double *pdfs, long long nCells, int nFluid, d
 int lbmh_pad_cells(int nCells, int pdfBytes, const char *padStr);
 int lbmh_list_build(const LatticeDesc *ld, int pull, const int blk[3], int nCells,
                     uint32_t *grid, uint32_t *coords, uint32_t *adj);
+
+/* ---- Batched domains (no counterpart in the reference) ----
+ * Many independent porous domains of uneven size, each with its own list
+ * layout (push adjacency as the list AA kernel, node range padded to tiles of
+ * 256 nodes) in its own device allocations, advanced together by one
+ * persistent even and one persistent odd launch per step pair over a device
+ * tile table. Storage fp32 (1) or fp16 deviations (2), FP32 arithmetic. The
+ * kernels read the table from device memory, so CUDA graphs captured for a
+ * step count stay valid as domains are admitted and retired. */
+void *lbm_batch_create(int storage, double budgetGB, int maxDomains);
+void lbm_batch_destroy(void *batch);
+/* Admits a domain at rest (f = w); returns its slot, -1 if the HBM budget is
+ * exhausted, -2 if every slot is taken, other negatives on errors. */
+int lbm_batch_add(void *batch, const LatticeDesc *ld, double omega, double lambda, double xforce);
+int lbm_batch_remove(void *batch, int slot);
+int lbm_batch_reset(void *batch, int slot);
+/* Enqueues nsteps (rounded up to even) steps of every active domain; with
+ * use_graph the sequence is replayed from a captured CUDA graph. */
+int lbm_batch_step(void *batch, int nsteps, int use_graph);
+int lbm_batch_sync(void *batch);
+/* FP64 {rho, jx, jy, jz} sums of every slot: out has maxDomains * 4 doubles. */
+int lbm_batch_moments(void *batch, double *out);
+int lbm_batch_get_field(void *batch, int slot, double *out);
+int lbm_batch_set_field(void *batch, int slot, const double *in);
+/* which: 0 even, 1 odd, 2 both; threads 64/128/256 (nodes per thread =
+ * 256 / threads); blocks = persistent grid size. */
+int lbm_batch_set_launch(void *batch, int which, int threads, int blocks);
+void lbm_batch_get_launch(void *batch, int *out6);
+int lbm_batch_time_steps(void *batch, int nsteps, double *ms);
+/* Autotuner over block size x nodes per thread x persistent grid (rows of
+ * {which, threads, nodesPerThread, blocks, ms}); keeps the fastest. */
+int lbm_batch_tune(void *batch, int trialSteps, double *results, int maxRows);
+size_t lbm_batch_bytes_used(void *batch);
+long long lbm_batch_launches(void *batch);
+int lbm_batch_active_domains(void *batch);
+int lbm_batch_fluid_nodes(void *batch, int slot);
+const char *lbm_batch_last_error(void);
 
 #ifdef __cplusplus
 }

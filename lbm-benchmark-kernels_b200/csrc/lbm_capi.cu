@@ -66,6 +66,8 @@ struct Gpu {
   int nFluid, nCells;
   int cur;  // pull: index of the current grid (0 = dF, 1 = dG)
 
+  double* dMomOut;  // 4 doubles for lbm_b200_instance_moments (allocated on first use)
+
   // last Kernel call
   double lastDeviceMs;
   long lastLaunches;
@@ -252,6 +254,7 @@ lbm::AaArgs aa_args(Gpu* g) {
   a.perX = g->per[0];
   a.perY = g->per[1];
   a.perZ = g->per[2];
+  for (int d = 0; d < Q; ++d) a.plane[d] = g->dF + d * g->dstride;
   return a;
 }
 
@@ -289,7 +292,7 @@ long enqueue_steps(Gpu* g, const lbm::Trt<double>& t, int n, cudaEvent_t* ev = n
   };
   if (g->kind == kAa) {
     lbm::AaArgs a = aa_args(g);
-    const bool interior = lbm::aa_has_interior(a);
+    const bool interior = lbm::aa_has_interior(a), shell = lbm::aa_shell_cells(a) > 0;
     for (int it = 0; it < n; it += 2) {
       mark();
       lbm::aa_even_fp64(a, t, g->stream);
@@ -299,9 +302,11 @@ long enqueue_steps(Gpu* g, const lbm::Trt<double>& t, int n, cudaEvent_t* ev = n
         lbm::aa_odd_interior_fp64(a, t, g->stream);
         ++k;
       }
-      mark();
-      lbm::aa_odd_face_fp64(a, t, g->stream);
-      ++k;
+      if (shell) {
+        mark();
+        lbm::aa_odd_face_fp64(a, t, g->stream);
+        ++k;
+      }
       g->iteration = it + 1;
     }
   } else if (g->kind == kListAa && g->storage != lbm::kStoreF64) {
@@ -343,7 +348,11 @@ long enqueue_steps(Gpu* g, const lbm::Trt<double>& t, int n, cudaEvent_t* ev = n
 
 long launches_for(Gpu* g, int n) {
   if (g->kind == kListPull) return n;
-  const long perPair = g->kind == kAa ? (lbm::aa_has_interior(aa_args(g)) ? 3 : 2) : 2;
+  long perPair = 2;
+  if (g->kind == kAa) {
+    const lbm::AaArgs a = aa_args(g);
+    perPair = 1 + (lbm::aa_has_interior(a) ? 1 : 0) + (lbm::aa_shell_cells(a) > 0 ? 1 : 0);
+  }
   return perPair * ((n + 1) / 2);
 }
 
@@ -552,6 +561,7 @@ void gpu_free(KernelData** kernelData) {
   cudaFree(g->dLink);
   cudaFree(g->dAdj);
   cudaFree(g->dErr);
+  cudaFree(g->dMomOut);
   cudaFreeHost(g->mirror);
   cudaFreeHost(g->rawStage);
   cudaEventDestroy(g->ev0);
@@ -678,6 +688,22 @@ int lbm_b200_device_state(KernelData* kd, double** pdfs, long long* nCells, int*
   if (nFluid) *nFluid = g->nFluid;
   if (stream) *stream = g->stream;
   return 0;
+}
+
+int lbm_b200_moments_device(const double* pdfs, long long nCells, int nFluid, double* out_device, void* stream);
+
+int lbm_b200_instance_moments(KernelData* kd, double* out) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (g->kind == kAa || g->storage != lbm::kStoreF64) return -1;
+  if (g->dirty) upload_if_dirty(g);
+  if (g->dMomOut == nullptr) {
+    cudaError_t e = cudaMalloc(&g->dMomOut, 4 * sizeof(double));
+    if (e != cudaSuccess) { g_lastError = cudaGetErrorString(e); return (int)e; }
+  }
+  int rc = lbm_b200_moments_device(current_grid(g), g->nCells, g->nFluid, g->dMomOut, g->stream);
+  if (rc) return rc;
+  cudaError_t e = cudaMemcpy(out, g->dMomOut, 4 * sizeof(double), cudaMemcpyDeviceToHost);
+  return (int)e;
 }
 
 int lbm_b200_set_device(int device) {

@@ -34,6 +34,7 @@ struct AaArgs {
   int nX, nY, nZ;
   int xs, pitch;
   int perX, perY, perZ;
+  double* plane[Q];  // f + d * dstride: one address add per access from the parameter bank
 };
 
 // ---------------------------------------------------------------------------

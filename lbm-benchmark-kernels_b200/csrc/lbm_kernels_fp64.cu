@@ -79,45 +79,52 @@ __global__ void __launch_bounds__(128) k_aa_even_fp64(const AaArgs a, const Trt<
 // (x + c_i, i) with the increment of i, or -- bounced back at a wall -- to
 // its own slot (x, inv(i)) with the increment of inv(i).
 //
-// Two kernels share the step. The interior kernel takes the cells off every
-// domain face: no link of theirs can leave the domain, so each address is a
-// select between the neighbour's slot and the node's own slot, and the 19
-// loads are issued together. The face kernel takes the one-cell shell: links
-// that leave the domain wrap periodically on every crossed axis, or, at a
-// non-periodic face, go to the ghost layer (an "open" link), as in the
-// reference.
+// Two kernels share the step. The interior kernel takes every cell off the x
+// and y faces -- and off the z faces too unless z is periodic: links of these
+// cells leave the domain at most through a periodic z face, which is a fixed
+// offset of -/+ nZ cells, so each address is a select between the
+// neighbour's slot and the node's own slot and the 19 loads are issued
+// together. The face kernel takes the remaining shell: links that leave the
+// domain wrap periodically on every crossed axis, or, at a non-periodic face,
+// go to the ghost layer (an "open" link), as in the reference.
 __global__ void __launch_bounds__(128) k_aa_odd_interior_fp64(const AaArgs a, const Trt<double> t) {
-  const int z = 1 + blockIdx.x * 32 + threadIdx.x;
+  const int zLo = a.perZ ? 0 : 1, zHi = a.perZ ? a.nZ - 1 : a.nZ - 2;
+  const int z = zLo + blockIdx.x * 32 + threadIdx.x;
   const int y = 1 + blockIdx.y * 4 + threadIdx.y;
   const int x = 1 + blockIdx.z;
-  if (z > a.nZ - 2 || y > a.nY - 2) return;
+  if (z > zHi || y > a.nY - 2) return;
   const int c = aa_cell(a, x, y, z);
   const uint32_t w = __ldg(a.link + c);
   if (!(w & kFluidBit)) return;
-  const long long S = a.dstride;
-  double* const f = a.f;
-  double* const fs = launder(f);
+  // the periodic z wrap, decided once per cell: a link with c_z = -1 leaving
+  // through z = 0 moves +nZ cells, one with c_z = +1 through z = nZ-1 moves -nZ
+  const int wrapDown = z == 0 ? a.nZ : 0, wrapUp = z == a.nZ - 1 ? -a.nZ : 0;
+  auto nbr = [&](int d) -> int {
+    return c + aa_off(a, d) + (cz(d) < 0 ? wrapDown : (cz(d) > 0 ? wrapUp : 0));
+  };
   auto load = [&](int d) -> double {
-    if (d == DC) return f[DC * S + c] + t.force[DC];
+    if (d == DC) return a.plane[DC][c] + t.force[DC];
     const int j = inv(d);
     const bool rev = (w >> j) & 1u;
-    return f[rev ? d * S + c : j * S + c + aa_off(a, j)] + t.force[d];
+    return (rev ? a.plane[d] + c : a.plane[j] + nbr(j))[0] + t.force[d];
   };
+  // store addresses are formed from laundered plane pointers, apart from the
+  // load addresses, so those need not stay live across the collision
   auto store = [&](int d, double v) {
     if (d == DC) {
-      fs[DC * S + c] = v + t.force[DC];
+      launder(a.plane[DC])[c] = v + t.force[DC];
       return;
     }
     const int j = inv(d);
     const bool rev = (w >> d) & 1u;
-    fs[rev ? j * S + c : d * S + c + aa_off(a, d)] = v + (rev ? t.force[j] : t.force[d]);
+    (rev ? launder(a.plane[j]) + c : launder(a.plane[d]) + nbr(d))[0] = v + (rev ? t.force[j] : t.force[d]);
   };
   trt_update(t, load, store);
 }
 
 // Cell of shell index i: the x faces (all y, z), then the y faces (inner x,
-// all z), then the z faces (inner x and y). A one-cell-thin axis has a single
-// face.
+// all z), then -- when z is not periodic -- the z faces (inner x and y). A
+// one-cell-thin axis has a single face.
 __device__ __forceinline__ void aa_shell_cell(const AaArgs& a, long long i, int& x, int& y, int& z) {
   const long long nY = a.nY, nZ = a.nZ;
   const long long sx = a.nX > 1 ? 2 : 1, sy = a.nY > 1 ? 2 : 1;
@@ -185,10 +192,10 @@ __global__ void __launch_bounds__(128) k_aa_odd_face_fp64(const AaArgs a, const 
 long long aa_shell_cells(const AaArgs& a) {
   const long long sx = a.nX > 1 ? 2 : 1, sy = a.nY > 1 ? 2 : 1, sz = a.nZ > 1 ? 2 : 1;
   const long long mx = a.nX > 2 ? a.nX - 2 : 0, my = a.nY > 2 ? a.nY - 2 : 0;
-  return sx * a.nY * a.nZ + sy * mx * a.nZ + sz * mx * my;
+  return sx * a.nY * a.nZ + sy * mx * a.nZ + (a.perZ ? 0 : sz * mx * my);
 }
 
-bool aa_has_interior(const AaArgs& a) { return a.nX > 2 && a.nY > 2 && a.nZ > 2; }
+bool aa_has_interior(const AaArgs& a) { return a.nX > 2 && a.nY > 2 && (a.perZ || a.nZ > 2); }
 
 static dim3 aa_grid(const AaArgs& a) { return dim3((a.nZ + 31) / 32, (a.nY + 3) / 4, a.nX); }
 
@@ -198,12 +205,13 @@ void aa_even_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
 
 void aa_odd_interior_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
   if (!aa_has_interior(a)) return;
-  k_aa_odd_interior_fp64<<<dim3((a.nZ - 2 + 31) / 32, (a.nY - 2 + 3) / 4, a.nX - 2), dim3(32, 4), 0, s>>>(a, t);
+  const int nz = a.perZ ? a.nZ : a.nZ - 2;
+  k_aa_odd_interior_fp64<<<dim3((nz + 31) / 32, (a.nY - 2 + 3) / 4, a.nX - 2), dim3(32, 4), 0, s>>>(a, t);
 }
 
 void aa_odd_face_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
   const long long n = aa_shell_cells(a);
-  k_aa_odd_face_fp64<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a, t, n);
+  if (n > 0) k_aa_odd_face_fp64<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a, t, n);
 }
 
 // ---------------------------------------------------------------------------

@@ -292,3 +292,135 @@ def list_build(lattice, pull, blk=(0, 0, 0), pad=None):
                            grid.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), None,
                            adj.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
     return grid, adj[: nf * 18], nf, n_cells
+
+
+# ---------------------------------------------------------------------------
+# Batched domains (lbm_batch_* in include/lbm_b200.h)
+
+STORAGE = {"fp32": 1, "fp16": 2}
+
+
+def _batch_lib():
+    L = lib()
+    if not getattr(L, "_batch_sigs", False):
+        L.lbm_batch_create.restype = ctypes.c_void_p
+        L.lbm_batch_create.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int]
+        for name in ("lbm_batch_destroy", "lbm_batch_add", "lbm_batch_remove", "lbm_batch_reset", "lbm_batch_step",
+                     "lbm_batch_sync", "lbm_batch_moments", "lbm_batch_get_field", "lbm_batch_set_field",
+                     "lbm_batch_set_launch", "lbm_batch_get_launch", "lbm_batch_time_steps", "lbm_batch_tune",
+                     "lbm_batch_bytes_used", "lbm_batch_launches", "lbm_batch_active_domains",
+                     "lbm_batch_fluid_nodes"):
+            getattr(L, name).argtypes = None
+        L.lbm_batch_add.argtypes = [ctypes.c_void_p, ctypes.POINTER(LatticeDesc), ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double]
+        L.lbm_batch_bytes_used.restype = ctypes.c_size_t
+        L.lbm_batch_launches.restype = ctypes.c_longlong
+        L.lbm_batch_last_error.restype = ctypes.c_char_p
+        L._batch_sigs = True
+    return L
+
+
+class Batch:
+    """Many independent domains advanced by one persistent launch per step."""
+
+    def __init__(self, storage="fp32", budget_gb=150.0, max_domains=1024):
+        self.L = _batch_lib()
+        self.max_domains = max_domains
+        self.h = self.L.lbm_batch_create(STORAGE[storage], ctypes.c_double(budget_gb), max_domains)
+        if not self.h:
+            raise RuntimeError(self.L.lbm_batch_last_error().decode())
+        self.h = ctypes.c_void_p(self.h)
+        self.lattices = {}
+
+    def add(self, lattice, omega=1.0, lam=3.0 / 16.0, xforce=1e-5):
+        slot = self.L.lbm_batch_add(self.h, ctypes.byref(lattice.desc), omega, lam, xforce)
+        if slot >= 0:
+            self.lattices[slot] = lattice
+        return slot
+
+    def remove(self, slot):
+        rc = self.L.lbm_batch_remove(self.h, slot)
+        self.lattices.pop(slot, None)
+        return rc
+
+    def step(self, n, graph=True):
+        rc = self.L.lbm_batch_step(self.h, int(n), int(bool(graph)))
+        if rc:
+            raise RuntimeError("batch step failed: %s" % self.L.lbm_batch_last_error().decode())
+
+    def sync(self):
+        rc = self.L.lbm_batch_sync(self.h)
+        if rc:
+            raise RuntimeError("batch sync failed: %s" % self.L.lbm_batch_last_error().decode())
+
+    def moments(self):
+        out = np.zeros(self.max_domains * 4)
+        rc = self.L.lbm_batch_moments(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        if rc:
+            raise RuntimeError("batch moments failed: %s" % self.L.lbm_batch_last_error().decode())
+        return out.reshape(-1, 4)
+
+    def get_field(self, slot):
+        lat = self.lattices[slot]
+        out = np.full(lat.mask.size * Q, np.nan)
+        rc = self.L.lbm_batch_get_field(self.h, slot, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        assert rc == 0
+        return out.reshape(-1, Q)
+
+    def set_field(self, slot, pdfs):
+        pdfs = np.ascontiguousarray(pdfs, dtype=np.float64).reshape(-1)
+        rc = self.L.lbm_batch_set_field(self.h, slot, pdfs.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        assert rc == 0
+
+    def time_steps(self, n):
+        ms = ctypes.c_double(0.0)
+        rc = self.L.lbm_batch_time_steps(self.h, int(n), ctypes.byref(ms))
+        if rc:
+            raise RuntimeError(self.L.lbm_batch_last_error().decode())
+        return ms.value
+
+    def tune(self, trial_steps=10):
+        rows = np.zeros((64, 5))
+        n = self.L.lbm_batch_tune(self.h, int(trial_steps), rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 64)
+        return rows[:n]
+
+    def launch(self):
+        out = (ctypes.c_int * 6)()
+        self.L.lbm_batch_get_launch(self.h, out)
+        return {"even": {"threads": out[0], "nodes_per_thread": out[1], "blocks": out[2]},
+                "odd": {"threads": out[3], "nodes_per_thread": out[4], "blocks": out[5]}}
+
+    def set_launch(self, which, threads, blocks):
+        assert self.L.lbm_batch_set_launch(self.h, {"even": 0, "odd": 1, "both": 2}[which], threads, blocks) == 0
+
+    @property
+    def bytes_used(self):
+        return self.L.lbm_batch_bytes_used(self.h)
+
+    def fluid_nodes(self, slot):
+        return self.L.lbm_batch_fluid_nodes(self.h, slot)
+
+    def close(self):
+        if self.h:
+            self.L.lbm_batch_destroy(self.h)
+            self.h = None
+
+
+def spheres(dims, seed, porosity, rmin, rmax, rsa_attempts=20000):
+    """Seeded periodic sphere packing (lbm_geo_spheres): (Lattice, stats)."""
+    L = lib()
+    L.lbm_geo_spheres.argtypes = [ctypes.c_int * 3, ctypes.c_uint64, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_int, ctypes.POINTER(LatticeDesc),
+                                  ctypes.POINTER(ctypes.c_double)]
+    ld = LatticeDesc()
+    st = (ctypes.c_double * 4)()
+    rc = L.lbm_geo_spheres((ctypes.c_int * 3)(*dims), int(seed), porosity, rmin, rmax, rsa_attempts,
+                           ctypes.byref(ld), st)
+    if rc:
+        raise ValueError("sphere packing rejected its arguments")
+    n = dims[0] * dims[1] * dims[2]
+    mask = np.ctypeslib.as_array(ld.Lattice, shape=(n,)).copy()
+    ctypes.CDLL(None).free(ctypes.cast(ld.Lattice, ctypes.c_void_p))
+    lat = Lattice(mask, dims, (1, 1, 1), "spheres")
+    return lat, {"porosity": st[0], "spheres_rsa": int(st[1]), "spheres_overlap": int(st[2]),
+                 "jam_porosity": st[3]}

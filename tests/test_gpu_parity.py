@@ -157,3 +157,18 @@ def test_mass_conserved_periodic_fluid():
     for kname, _, _ in KERNELS:
         g, _ = _run_gpu(kname, lat, init, 1.5, 0.0, 50)
         assert abs(g.sum() - init.sum()) / init.sum() < 1e-13
+
+
+def test_bounded_wait_reports_instead_of_hanging():
+    import ctypes
+    L = lbmb200.lib()
+    st = ctypes.c_int(0)
+    assert L.lbm_b200_selftest_bounded_wait(ctypes.c_uint(1 << 16), ctypes.byref(st)) == 0
+    assert st.value == 2
+    # the context is still usable afterwards
+    lat = lbmb200.geometry("fluid", (8, 8, 8), (1, 1, 1))
+    inst = lbmb200.kernel("cuda-list-aa-pv-soa").init(lat)
+    try:
+        inst.run(lbmb200.case(iterations=2))
+    finally:
+        inst.deinit()
