@@ -277,6 +277,8 @@ def section_batched(args, dist, peak):
             raise RuntimeError("the domains do not fit the HBM budget")
         nodes = sum(l.n_fluid for l in lats)
         rows = b.tune(trial_steps=6)
+        print("batched tuner rows {which, threads, nodes/thread, blocks (0 = one per tile), ms}:\n"
+              + "\n".join(" ".join("%g" % v for v in r) for r in rows), file=sys.stderr)
         cfg = b.launch()
         b.step(100, graph=True)  # capture and warm the graph
         b.sync()

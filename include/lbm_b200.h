@@ -161,6 +161,18 @@ double lbm_verify(LatticeDesc *ld, KernelData *kd, CaseData *cd, int write_file)
 /* KernelDensity (src/Kernel.c:209-254): mean density over the fluid nodes. */
 double lbm_density(KernelData *kd, LatticeDesc *ld);
 
+/* VtkWrite (src/Vtk.c:51-245): legacy VTK file of the current state through
+ * GetNode -- cell flags, density, velocity (with the F/2 shift of the
+ * reference's VERIFICATION builds) -- byte for byte the reference's format.
+ * lbm_vtk_write writes vtk/file-%04d.vtk (creating vtk/), as the reference;
+ * lbm_vtk_write_file writes `path`. Return 0 or -1. The CUDA rows' Kernel
+ * writes these files itself when cd->VtkOutput is set: before the first step
+ * (label -1), after each step pair (AA forms) or step (pull) whose first step
+ * index is a multiple of cd->VtkModulus (label: that index), and after the
+ * last step (label MaxIterations). */
+int lbm_vtk_write(LatticeDesc *ld, KernelData *kd, CaseData *cd, int iteration);
+int lbm_vtk_write_file(LatticeDesc *ld, KernelData *kd, CaseData *cd, int iteration, const char *path);
+
 /* ---- B200 additions with no counterpart in the reference ---- */
 
 /* Seeded packing of solid spheres in a fully periodic box: random sequential
@@ -234,6 +246,17 @@ int lbm_b200_moments_device(const double *pdfs, long long nCells, int nFluid, do
  * full-array kernel or reduced storage, or a CUDA error code. */
 int lbm_b200_instance_moments(KernelData *kd, double *out);
 
+/* Checkpoint / restart of an instance (no counterpart in the reference):
+ * _save writes the current state -- a header (kernel, storage, lattice
+ * dimensions and periodicity, step parity, Lambda; host byte order) and the
+ * PDF array exactly as the device holds it, with an FNV-1a checksum; pending
+ * SetNode edits are part of the state. _load restores it into an instance of
+ * the same kernel, storage, lattice and Lambda, so that the run continues
+ * bit for bit. Return 0; -1 I/O error; -2 the file does not match the
+ * instance; -3 checksum mismatch (state unchanged); or a CUDA error code. */
+int lbm_b200_checkpoint_save(KernelData *kd, const char *path);
+int lbm_b200_checkpoint_load(KernelData *kd, const char *path);
+
 /* Last CUDA error string seen by the library ("" if none). */
 const char *lbm_b200_last_error(void);
 
@@ -272,11 +295,13 @@ int lbmh_list_build(const LatticeDesc *ld, int pull, const int blk[3], int nCell
 /* ---- Batched domains (no counterpart in the reference) ----
  * Many independent porous domains of uneven size, each with its own list
  * layout (push adjacency as the list AA kernel, node range padded to tiles of
- * 256 nodes) in its own device allocations, advanced together by one
- * persistent even and one persistent odd launch per step pair over a device
- * tile table. Storage fp32 (1) or fp16 deviations (2), FP32 arithmetic. The
- * kernels read the table from device memory, so CUDA graphs captured for a
- * step count stay valid as domains are admitted and retired. */
+ * 256 nodes) in its own device allocations, advanced together by one even and
+ * one odd launch per step pair over a device table of tile records (a
+ * persistent grid, or one block per tile). Storage fp32 (1) or fp16
+ * deviations (2), FP32 arithmetic. The kernels read the table and its length
+ * from device memory, so CUDA graphs captured for a step count stay valid as
+ * domains are admitted and retired (until the table outgrows its allocation
+ * or the one-block-per-tile grid, when they are captured again). */
 void *lbm_batch_create(int storage, double budgetGB, int maxDomains);
 void lbm_batch_destroy(void *batch);
 /* Admits a domain at rest (f = w); returns its slot, -1 if the HBM budget is
@@ -293,13 +318,20 @@ int lbm_batch_moments(void *batch, double *out);
 int lbm_batch_get_field(void *batch, int slot, double *out);
 int lbm_batch_set_field(void *batch, int slot, const double *in);
 /* which: 0 even, 1 odd, 2 both; threads 64/128/256 (nodes per thread =
- * 256 / threads); blocks = persistent grid size. */
+ * 256 / threads); blocks = persistent grid size, 0 = one block per tile. */
 int lbm_batch_set_launch(void *batch, int which, int threads, int blocks);
 void lbm_batch_get_launch(void *batch, int *out6);
 int lbm_batch_time_steps(void *batch, int nsteps, double *ms);
-/* Autotuner over block size x nodes per thread x persistent grid (rows of
- * {which, threads, nodesPerThread, blocks, ms}); keeps the fastest. */
+/* Autotuner over block size x nodes per thread x grid (2..6 persistent
+ * blocks per SM, or 0 = one block per tile); rows of {which, threads,
+ * nodesPerThread, blocks, ms}; keeps the fastest. */
 int lbm_batch_tune(void *batch, int trialSteps, double *results, int maxRows);
+/* Checkpoint / restart of one resident domain: its PDFs in the batch's
+ * storage format plus its lattice size and relaxation parameters. _load
+ * needs an active slot admitted from the same lattice with the same omega,
+ * Lambda and force. Return codes as lbm_b200_checkpoint_save / _load. */
+int lbm_batch_checkpoint_save(void *batch, int slot, const char *path);
+int lbm_batch_checkpoint_load(void *batch, int slot, const char *path);
 size_t lbm_batch_bytes_used(void *batch);
 long long lbm_batch_launches(void *batch);
 int lbm_batch_active_domains(void *batch);

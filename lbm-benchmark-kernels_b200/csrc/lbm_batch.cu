@@ -61,6 +61,9 @@ struct Batch {
   cudaStream_t stream = nullptr;
   lbm::BatchDomain* dDoms = nullptr;
   int* dTileDom = nullptr;
+  lbm::BatchTile* dTiles = nullptr;  // tile records, capacity tileCap
+  int tileCap = 0;
+  int gridTiles = 0;  // grid of the one-block-per-tile launches (>= nTiles)
   int* dNTiles = nullptr;
   int* dErr = nullptr;
   double* dPartials = nullptr;
@@ -77,6 +80,7 @@ lbm::BatchArgs args_of(const Batch* b, const lbm::BatchLaunch& l) {
   lbm::BatchArgs a;
   a.doms = b->dDoms;
   a.tileDom = b->dTileDom;
+  a.tiles = b->dTiles;
   a.nTiles = b->dNTiles;
   a.err = b->dErr;
   a.storage = b->storage;
@@ -85,8 +89,14 @@ lbm::BatchArgs args_of(const Batch* b, const lbm::BatchLaunch& l) {
   return a;
 }
 
-// Rebuilds the tile table and the per-domain tile ranges after a change of
-// membership (stream-ordered uploads).
+void drop_graphs(Batch* b) {
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+}
+
+// Rebuilds the tile table, the per-domain tile ranges and the tile records
+// after a change of membership (stream-ordered uploads, then a device pass
+// that fills the records).
 int publish(Batch* b) {
   b->tileDomHost.clear();
   std::vector<int> start(b->maxSlots, 0), count(b->maxSlots, 0);
@@ -104,50 +114,97 @@ int publish(Batch* b) {
   if (b->nTiles)
     BCK(cudaMemcpyAsync(b->dTileDom, b->tileDomHost.data(), sizeof(int) * b->nTiles, cudaMemcpyHostToDevice,
                         b->stream));
+  if (b->nTiles > b->tileCap) {
+    // records are reallocated: graphs captured with the old table go
+    BCK(cudaStreamSynchronize(b->stream));
+    drop_graphs(b);
+    cudaFree(b->dTiles);
+    b->dTiles = nullptr;
+    b->tileCap = 0;
+    const int cap = std::min(b->maxTiles, std::max(b->nTiles + b->nTiles / 2, 1024));
+    BCK(cudaMalloc(&b->dTiles, sizeof(lbm::BatchTile) * (size_t)cap));
+    b->tileCap = cap;
+  }
+  // the grid of one-block-per-tile launches keeps some headroom, so that
+  // graphs survive admissions; it is resized (and graphs dropped) when the
+  // table outgrows it or shrinks below half of it
+  if (b->nTiles > b->gridTiles || b->nTiles < b->gridTiles / 2) {
+    const int g = std::max(b->nTiles + b->nTiles / 8, 64);
+    if (g != b->gridTiles) {
+      drop_graphs(b);
+      b->gridTiles = g;
+    }
+  }
   BCK(cudaMemcpyAsync(b->dNTiles, &b->nTiles, sizeof(int), cudaMemcpyHostToDevice, b->stream));
   BCK(cudaMemcpyAsync(b->dDomTileStart, start.data(), sizeof(int) * b->maxSlots, cudaMemcpyHostToDevice, b->stream));
   BCK(cudaMemcpyAsync(b->dDomTileCount, count.data(), sizeof(int) * b->maxSlots, cudaMemcpyHostToDevice, b->stream));
+  lbm::batch_build_tiles(b->dDoms, b->dTileDom, b->nTiles, b->dTiles, b->stream);
+  BCK(cudaGetLastError());
   // the host vectors above are read by the copies: wait before they go away
   BCK(cudaStreamSynchronize(b->stream));
   return 0;
 }
 
 int enqueue(Batch* b, int nsteps) {
+  if (b->nTiles == 0) return 0;
   const lbm::BatchArgs ae = args_of(b, b->evenL), ao = args_of(b, b->oddL);
   for (int it = 0; it < nsteps; it += 2) {
-    lbm::batch_even_lp(ae, b->evenL, b->stream);
-    lbm::batch_odd_lp(ao, b->oddL, b->stream);
+    lbm::batch_even_lp(ae, b->evenL, b->evenL.blocks ? b->evenL.blocks : b->gridTiles, b->stream);
+    lbm::batch_odd_lp(ao, b->oddL, b->oddL.blocks ? b->oddL.blocks : b->gridTiles, b->stream);
     b->launches += 2;
   }
   BCK(cudaGetLastError());
   return 0;
 }
 
-void drop_graphs(Batch* b) {
-  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
-  b->graphs.clear();
-}
-
 size_t domain_bytes(const Batch* b, long long nCells) {
   return (size_t)nCells * Q * b->elemBytes + (size_t)nCells * QM * 4;
 }
 
-lbm::Trt<float> trt_of(double omega, double lambda, double xforce) {
-  lbm::Trt<float> t;
-  const double w0 = 1.0 / 3.0, w1 = 1.0 / 18.0, w2 = 1.0 / 36.0;
+lbm::TrtW trt_of(double omega, double lambda, double xforce) {
+  lbm::TrtW t;
   t.omegaEven = (float)omega;
   t.omegaOdd = (float)(1.0 / (0.5 + lambda / (1.0 / omega - 0.5)));
-  t.w0 = (float)w0;
-  t.w1 = (float)w1;
-  t.w2 = (float)w2;
-  t.w1x3 = (float)(w1 * 3.0);
-  t.w2x3 = (float)(w2 * 3.0);
-  t.w1nh = (float)(w1 * 9.0 / 2.0);
-  t.w2nh = (float)(w2 * 9.0 / 2.0);
-  for (int d = 0; d < Q; ++d) t.force[d] = (float)(3.0 * weight_of(d) * lbm::cx(d) * xforce);
+  t.fx1 = (float)(3.0 * (1.0 / 18.0) * xforce);
+  t.fx2 = (float)(3.0 * (1.0 / 36.0) * xforce);
   return t;
 }
 
+// Domain checkpoint: header (host byte order), then the slot's PDF array as
+// the device holds it (storage format, tile padding included).
+struct DomCkpt {
+  char magic[8];  // "LBMBDOM1"
+  int32_t storage, nFluid;
+  int32_t dims[3], reserved;
+  int64_t nCells;
+  double omega, lambda, xforce;
+  uint64_t checksum;
+};
+const char kDomMagic[8] = {'L', 'B', 'M', 'B', 'D', 'O', 'M', '1'};
+
+uint64_t dom_fnv1a64(const void* data, size_t n) {
+  const unsigned char* p = static_cast<const unsigned char*>(data);
+  uint64_t h = 1469598103934665603ull;
+  for (size_t k = 0; k < n; ++k) {
+    h ^= p[k];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+DomCkpt dom_header_of(const Batch* b, const DomainSlot& d) {
+  DomCkpt c;
+  std::memset(&c, 0, sizeof(c));
+  std::memcpy(c.magic, kDomMagic, 8);
+  c.storage = b->storage;
+  c.nFluid = d.dev.nFluid;
+  for (int i = 0; i < 3; ++i) c.dims[i] = d.dims[i];
+  c.nCells = d.dev.nCells;
+  c.omega = d.omega;
+  c.lambda = d.lambda;
+  c.xforce = d.xforce;
+  return c;
+}
 }  // namespace
 
 extern "C" {
@@ -186,7 +243,7 @@ void* lbm_batch_create(int storage, double budgetGB, int maxDomains) {
     delete b;
     return nullptr;
   }
-  b->evenL.blocks = b->oddL.blocks = 2 * b->numSMs;
+  b->evenL.blocks = b->oddL.blocks = 0;  // one block per tile until tuned
   return b;
 }
 
@@ -201,6 +258,7 @@ void lbm_batch_destroy(void* h) {
   }
   cudaFree(b->dDoms);
   cudaFree(b->dTileDom);
+  cudaFree(b->dTiles);
   cudaFree(b->dNTiles);
   cudaFree(b->dErr);
   cudaFree(b->dPartials);
@@ -403,7 +461,7 @@ int lbm_batch_set_field(void* h, int slot, const double* in) {
 int lbm_batch_set_launch(void* h, int which, int threads, int blocks) {
   Batch* b = static_cast<Batch*>(h);
   if (threads != 64 && threads != 128 && threads != 256) return -1;
-  if (blocks <= 0) return -1;
+  if (blocks < 0) return -1;
   lbm::BatchLaunch l{threads, lbm::kBatchTileNodes / threads, blocks};
   if (which == 0 || which == 2) b->evenL = l;
   if (which == 1 || which == 2) b->oddL = l;
@@ -441,8 +499,8 @@ int lbm_batch_time_steps(void* h, int nsteps, double* ms) {
   return rc;
 }
 
-// Autotuner: times each (block size, nodes per thread, persistent grid)
-// candidate on the current batch for `trialSteps` steps, separately for the
+// Autotuner: times each (block size, nodes per thread, grid) candidate --
+// grids of 2..6 persistent blocks per SM, or one block per tile -- on the current batch for `trialSteps` steps, separately for the
 // even and the odd kernel (each candidate runs whole even/odd pairs with the
 // other kernel on its current setting), and keeps the fastest. Advances the
 // domains by the trial steps. results (optional): rows of
@@ -451,13 +509,13 @@ int lbm_batch_time_steps(void* h, int nsteps, double* ms) {
 int lbm_batch_tune(void* h, int trialSteps, double* results, int maxRows) {
   Batch* b = static_cast<Batch*>(h);
   const int threadsC[3] = {256, 128, 64};
-  const int perSM[5] = {1, 2, 3, 4, 6};
+  const int perSM[6] = {0, 2, 3, 4, 5, 6};  // 0: one block per tile
   int rows = 0;
   for (int which = 0; which < 2; ++which) {
     double bestMs = 1e300;
     lbm::BatchLaunch best = which == 0 ? b->evenL : b->oddL;
     for (int ti = 0; ti < 3; ++ti)
-      for (int pi = 0; pi < 5; ++pi) {
+      for (int pi = 0; pi < 6; ++pi) {
         lbm::BatchLaunch l{threadsC[ti], lbm::kBatchTileNodes / threadsC[ti], perSM[pi] * b->numSMs};
         if (which == 0) b->evenL = l; else b->oddL = l;
         double ms = 0.0;
@@ -474,6 +532,53 @@ int lbm_batch_tune(void* h, int trialSteps, double* results, int maxRows) {
   }
   drop_graphs(b);
   return std::min(rows, maxRows);
+}
+
+int lbm_batch_checkpoint_save(void* h, int slot, const char* path) {
+  Batch* b = static_cast<Batch*>(h);
+  if (slot < 0 || slot >= b->maxSlots || !b->slots[slot].active) return -1;
+  DomainSlot& d = b->slots[slot];
+  std::vector<unsigned char> raw((size_t)d.dev.nCells * Q * b->elemBytes);
+  BCK(cudaMemcpyAsync(raw.data(), d.pdfs, raw.size(), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  DomCkpt c = dom_header_of(b, d);
+  c.checksum = dom_fnv1a64(raw.data(), raw.size());
+  FILE* fh = std::fopen(path, "wb");
+  if (!fh) { g_batchError = "cannot open the checkpoint file"; return -1; }
+  const bool ok = std::fwrite(&c, sizeof(c), 1, fh) == 1 && std::fwrite(raw.data(), 1, raw.size(), fh) == raw.size();
+  if (std::fclose(fh) != 0 || !ok) { g_batchError = "writing the checkpoint file failed"; return -1; }
+  return 0;
+}
+
+int lbm_batch_checkpoint_load(void* h, int slot, const char* path) {
+  Batch* b = static_cast<Batch*>(h);
+  if (slot < 0 || slot >= b->maxSlots || !b->slots[slot].active) return -1;
+  DomainSlot& d = b->slots[slot];
+  FILE* fh = std::fopen(path, "rb");
+  if (!fh) { g_batchError = "cannot open the checkpoint file"; return -1; }
+  DomCkpt c;
+  const DomCkpt want = dom_header_of(b, d);
+  if (std::fread(&c, sizeof(c), 1, fh) != 1 || std::memcmp(c.magic, kDomMagic, 8) != 0) {
+    std::fclose(fh);
+    g_batchError = "not a domain checkpoint";
+    return -2;
+  }
+  bool same = c.storage == want.storage && c.nFluid == want.nFluid && c.nCells == want.nCells &&
+              c.omega == want.omega && c.lambda == want.lambda && c.xforce == want.xforce;
+  for (int i = 0; i < 3; ++i) same = same && c.dims[i] == want.dims[i];
+  if (!same) {
+    std::fclose(fh);
+    g_batchError = "the checkpoint belongs to a domain of another lattice, storage or relaxation";
+    return -2;
+  }
+  std::vector<unsigned char> raw((size_t)d.dev.nCells * Q * b->elemBytes);
+  const bool ok = std::fread(raw.data(), 1, raw.size(), fh) == raw.size();
+  std::fclose(fh);
+  if (!ok) { g_batchError = "the checkpoint file is truncated"; return -1; }
+  if (dom_fnv1a64(raw.data(), raw.size()) != c.checksum) { g_batchError = "checkpoint checksum mismatch"; return -3; }
+  BCK(cudaMemcpyAsync(d.pdfs, raw.data(), raw.size(), cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  return 0;
 }
 
 size_t lbm_batch_bytes_used(void* h) { return static_cast<Batch*>(h)->used; }

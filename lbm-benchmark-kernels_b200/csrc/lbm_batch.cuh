@@ -1,6 +1,6 @@
 // lbm_batch.cuh -- device side of the batched list AA form: many independent
-// porous domains of uneven size advanced by one persistent launch per time
-// step (no counterpart in the reference, which runs one domain per process).
+// porous domains of uneven size advanced by one launch per time step (a
+// persistent grid, or one block per tile) (no counterpart in the reference, which runs one domain per process).
 //
 // Each domain keeps its own list layout (fluid nodes numbered as the
 // reference's list kernels, adjacency with 32-bit PDF indices relative to the
@@ -24,12 +24,28 @@ struct BatchDomain {
   long long nCells;       // padded node count (a multiple of kBatchTileNodes)
   int nFluid;
   int tileStart;          // first tile of this domain in the tile table
-  Trt<float> trt;         // relaxation and body force of this domain
+  TrtW trt;               // relaxation rates and body force of this domain
 };
+
+// Everything a block needs to update one tile, built on the device from the
+// slot table whenever membership changes: the step kernels load one record
+// per tile, from an address that depends on the tile index alone, so the
+// record of a block's next tile is fetched while the current one is updated.
+struct BatchTile {
+  const uint32_t* adj;  // this tile's adjacency block, kBatchTileNodes x 18 entries
+  void* f;              // the domain's PDFs
+  int nCells;           // PDF plane stride of the domain (nCells * 19 < 2^32)
+  int n0;               // domain-local index of the tile's first node
+  int nValid;           // fluid nodes in the tile (0..kBatchTileNodes)
+  TrtW trt;             // relaxation rates and body force of the domain
+};
+constexpr int kTileWords = static_cast<int>(sizeof(BatchTile) / 4);  // one word per lane of a warp
+static_assert(sizeof(BatchTile) % 8 == 0 && kTileWords <= 32, "tile record layout");
 
 struct BatchArgs {
   const BatchDomain* doms;   // indexed by domain slot
   const int* tileDom;        // tile -> domain slot
+  const BatchTile* tiles;    // tile records (same order as tileDom)
   const int* nTiles;         // device word: number of tiles in the table
   int* err;
   int storage;               // kStoreF32 or kStoreF16
@@ -41,11 +57,16 @@ struct BatchArgs {
 struct BatchLaunch {
   int threads;         // block size
   int nodesPerThread;  // nodes each thread updates per tile
-  int blocks;          // persistent grid size
+  int blocks;          // persistent grid size; 0 = one block per tile
 };
 
-void batch_even_lp(const BatchArgs& a, const BatchLaunch& l, cudaStream_t s);
-void batch_odd_lp(const BatchArgs& a, const BatchLaunch& l, cudaStream_t s);
+// Builds the tile records of tiles [0, nTiles).
+void batch_build_tiles(const BatchDomain* doms, const int* tileDom, int nTiles, BatchTile* out, cudaStream_t s);
+
+// grid: the launch's block count (l.blocks, or the tile-grid size when
+// l.blocks is 0).
+void batch_even_lp(const BatchArgs& a, const BatchLaunch& l, int grid, cudaStream_t s);
+void batch_odd_lp(const BatchArgs& a, const BatchLaunch& l, int grid, cudaStream_t s);
 // FP64 sums {rho, jx, jy, jz} per tile (pass 1) and per domain slot (pass 2).
 void batch_moments(const BatchArgs& a, int maxTiles, double* tilePartials, const int* domTileStart,
                    const int* domTileCount, int nDomSlots, double* out, cudaStream_t s);

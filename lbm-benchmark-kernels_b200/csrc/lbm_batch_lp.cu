@@ -1,10 +1,11 @@
 // lbm_batch_lp.cu -- persistent list AA kernels over a batch of domains
 // (FP32 arithmetic on FP32 or FP16-deviation storage, as lbm_kernels_lp.cu).
 //
-// Every block walks the tile table with a grid stride. The odd step stages a
-// tile's adjacency (256 nodes x 18 entries, 18 KB, contiguous) into shared
-// memory with one bulk copy, double buffered: while a tile is relaxed, the
-// bulk copy of the block's next tile is already in flight.
+// Every block walks the tile records with a grid stride (one tile per block
+// when the grid covers the table). The odd step stages a tile's adjacency
+// (256 nodes x 18 entries, 18 KB, contiguous) into shared memory with one
+// bulk copy, double buffered: while a tile is relaxed, the bulk copy of the
+// block's next tile is already in flight.
 #include <cuda_fp16.h>
 
 #include "lbm_batch.cuh"
@@ -29,105 +30,235 @@ struct BStoreF16 {
   __device__ static T raw(float delta, int d) { return __float2half_rn(delta * scale(d)); }
 };
 
-template <class St>
-__device__ __forceinline__ void batch_even_node(const BatchDomain& D, int n) {
-  using T = typename St::T;
-  T* const f = static_cast<T*>(D.f) + n;
-  T* const fs = launder(f);
-  const long long S = D.nCells;
-  trt_update(D.trt, [&](int d) { return St::dev(f[d * S], d); },
-             [&](int d, float v) { fs[inv(d) * S] = St::raw(v, inv(d)); });
+// Warp 0 moves tile records: each lane loads one 32-bit word (the load of the
+// block's next-but-one record is issued before the current tile is updated
+// and consumed after it), then stores it to shared memory.
+__device__ __forceinline__ uint32_t tile_load(const BatchTile* tiles, int tile) {
+  const int lane = threadIdx.x;
+  return lane < kTileWords ? __ldg(reinterpret_cast<const uint32_t*>(tiles + tile) + lane) : 0u;
+}
+
+__device__ __forceinline__ void tile_store(BatchTile* dst, uint32_t w) {
+  const int lane = threadIdx.x;
+  if (lane < kTileWords) reinterpret_cast<uint32_t*>(dst)[lane] = w;
 }
 
 template <class St>
+__device__ __forceinline__ void batch_even_node(const BatchTile& T, int n) {
+  using T_ = typename St::T;
+  T_* const f = static_cast<T_*>(T.f) + n;
+  T_* const fs = launder(f);
+  const long long S = T.nCells;
+  trt_update(T.trt, [&](int d) { return St::dev(f[d * S], d); },
+             [&](int d, float v) { fs[inv(d) * S] = St::raw(v, inv(d)); });
+}
+
+// Grid-stride over the tiles; with one block per tile the loop runs once.
+template <class St>
 __global__ void __launch_bounds__(256) k_batch_even(const BatchArgs a) {
+  __shared__ __align__(16) BatchTile st[2];
   const int nT = *a.nTiles;
-  for (int tile = blockIdx.x; tile < nT; tile += gridDim.x) {
-    const BatchDomain& D = a.doms[a.tileDom[tile]];
-    const int base = (tile - D.tileStart) * kBatchTileNodes + threadIdx.x;
+  if (static_cast<int>(blockIdx.x) >= nT) return;
+  const bool warp0 = threadIdx.x < 32;
+  uint32_t r = 0;
+  if (warp0) {
+    r = tile_load(a.tiles, blockIdx.x);
+    tile_store(&st[0], r);
+    if (static_cast<int>(blockIdx.x + gridDim.x) < nT) r = tile_load(a.tiles, blockIdx.x + gridDim.x);
+  }
+  int it = 0;
+  for (int tile = blockIdx.x; tile < nT; tile += gridDim.x, ++it) {
+    const int buf = it & 1;
+    __syncthreads();  // st[buf] is written; every thread is done with st[buf ^ 1]
+    const int next = tile + gridDim.x;
+    if (warp0 && next < nT) {
+      tile_store(&st[buf ^ 1], r);
+      if (next + static_cast<int>(gridDim.x) < nT) r = tile_load(a.tiles, next + gridDim.x);
+    }
+    const BatchTile& T = st[buf];
     for (int k = 0; k < a.nodesPerThread; ++k) {
-      const int n = base + k * blockDim.x;
-      if (n < D.nFluid) batch_even_node<St>(D, n);
+      const int local = threadIdx.x + k * blockDim.x;
+      if (local < T.nValid) batch_even_node<St>(T, T.n0 + local);
     }
   }
 }
 
 template <class St>
-__device__ __forceinline__ void batch_odd_node(const BatchDomain& D, const uint32_t* e, int n) {
-  using T = typename St::T;
-  T* const f = static_cast<T*>(D.f);
-  const long long S = D.nCells;
-  const Trt<float>& t = D.trt;
-  auto load = [&](int d) -> float { return St::dev(d == DC ? f[DC * S + n] : f[e[inv(d)]], d) + t.force[d]; };
+__device__ __forceinline__ void batch_odd_node(const BatchTile& T, const uint32_t* e, int n) {
+  using T_ = typename St::T;
+  T_* const f = static_cast<T_*>(T.f);
+  const long long S = T.nCells;
+  const TrtW& t = T.trt;
+  auto load = [&](int d) -> float { return St::dev(d == DC ? f[DC * S + n] : f[e[inv(d)]], d) + t.force(d); };
   auto store = [&](int d, float v) {
     if (d == DC) {
-      f[DC * S + n] = St::raw(v + t.force[DC], DC);
+      f[DC * S + n] = St::raw(v + t.force(DC), DC);
       return;
     }
     const uint32_t dst = reinterpret_cast<const volatile uint32_t*>(e)[d];
     const int j = inv(d);
     const bool bounce = dst == static_cast<uint32_t>(j * S + n);
-    f[dst] = St::raw(v + (bounce ? t.force[j] : t.force[d]), d);
+    f[dst] = St::raw(v + (bounce ? t.force(j) : t.force(d)), d);
   };
   trt_update(t, load, store);
 }
 
 constexpr uint32_t kTileAdjBytes = kBatchTileNodes * QM * 4;
 
+// As k_batch_even, with the tile's adjacency staged into shared memory by one
+// bulk copy, double buffered: the copy of the block's next tile is issued
+// before the current tile is updated.
 template <class St>
 __global__ void __launch_bounds__(256) k_batch_odd(const BatchArgs a) {
   extern __shared__ __align__(128) uint32_t sadj[];  // 2 x kBatchTileNodes x 18
   __shared__ alignas(8) uint64_t bar[2];
+  __shared__ __align__(16) BatchTile st[2];
   const int nT = *a.nTiles;
-  if (blockIdx.x >= nT) return;
-
-  auto issue = [&](int tile, int buf) {
-    const BatchDomain& D = a.doms[a.tileDom[tile]];
-    const uint32_t* src = D.adj + static_cast<size_t>(tile - D.tileStart) * kBatchTileNodes * QM;
+  if (static_cast<int>(blockIdx.x) >= nT) return;
+  const bool warp0 = threadIdx.x < 32;
+  uint32_t r = 0;
+  auto issue = [&](int buf) {  // thread 0, once st[buf] holds the tile's record
     mbar_arrive_expect_tx(&bar[buf], kTileAdjBytes);
-    bulk_g2s(sadj + buf * kBatchTileNodes * QM, src, kTileAdjBytes, &bar[buf]);
+    bulk_g2s(sadj + buf * kBatchTileNodes * QM, st[buf].adj, kTileAdjBytes, &bar[buf]);
   };
-  if (threadIdx.x == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    issue(blockIdx.x, 0);
+  if (warp0) {
+    r = tile_load(a.tiles, blockIdx.x);
+    tile_store(&st[0], r);
+    __syncwarp();
+    if (threadIdx.x == 0) {
+      mbar_init(&bar[0], 1);
+      mbar_init(&bar[1], 1);
+      issue(0);
+    }
+    if (static_cast<int>(blockIdx.x + gridDim.x) < nT) r = tile_load(a.tiles, blockIdx.x + gridDim.x);
   }
-
   int it = 0;
   for (int tile = blockIdx.x; tile < nT; tile += gridDim.x, ++it) {
     const int buf = it & 1;
-    __syncthreads();  // every thread is done with buffer buf ^ 1 (the previous tile)
+    __syncthreads();  // st[buf] is written; every thread is done with buffers buf ^ 1
     const int next = tile + gridDim.x;
-    if (threadIdx.x == 0 && next < nT) issue(next, buf ^ 1);
+    if (warp0 && next < nT) {
+      tile_store(&st[buf ^ 1], r);
+      __syncwarp();
+      if (threadIdx.x == 0) issue(buf ^ 1);
+      if (next + static_cast<int>(gridDim.x) < nT) r = tile_load(a.tiles, next + gridDim.x);
+    }
     if (!mbar_wait_bounded(&bar[buf], (it >> 1) & 1)) {
-      if (threadIdx.x == 0) atomicOr(a.err, 1);
+      if (threadIdx.x == 0) {
+        atomicOr(a.err, 1);
+        // let the copy already issued for the next tile land before the
+        // block's shared memory is released
+        if (next < nT) mbar_wait_bounded(&bar[buf ^ 1], ((it + 1) >> 1) & 1);
+      }
       return;
     }
-    const BatchDomain& D = a.doms[a.tileDom[tile]];
+    const BatchTile& T = st[buf];
     const uint32_t* tileAdj = sadj + buf * kBatchTileNodes * QM;
     for (int k = 0; k < a.nodesPerThread; ++k) {
       const int local = threadIdx.x + k * blockDim.x;
-      const int n = (tile - D.tileStart) * kBatchTileNodes + local;
-      if (n < D.nFluid) batch_odd_node<St>(D, tileAdj + local * QM, n);
+      if (local < T.nValid) batch_odd_node<St>(T, tileAdj + local * QM, T.n0 + local);
     }
   }
-  // a block that exits early on a failed wait leaves its other copy unwaited;
-  // here every issued copy has been waited for
 }
 
-void batch_even_lp(const BatchArgs& a, const BatchLaunch& l, cudaStream_t s) {
-  if (a.storage == kStoreF16)
-    k_batch_even<BStoreF16><<<l.blocks, l.threads, 0, s>>>(a);
-  else
-    k_batch_even<BStoreF32><<<l.blocks, l.threads, 0, s>>>(a);
+// One block per tile: no loop state stays live across the node update, so
+// these take fewer registers (more resident blocks) than the persistent
+// kernels. NPT nodes per thread, blockDim = kBatchTileNodes / NPT.
+template <class St, int NPT>
+__global__ void __launch_bounds__(kBatchTileNodes / NPT) k_batch_even_tile(const BatchArgs a) {
+  __shared__ __align__(16) BatchTile st;
+  if (static_cast<int>(blockIdx.x) >= *a.nTiles) return;
+  if (threadIdx.x < 32) tile_store(&st, tile_load(a.tiles, blockIdx.x));
+  __syncthreads();
+#pragma unroll 1
+  for (int k = 0; k < NPT; ++k) {
+    const int local = threadIdx.x + k * (kBatchTileNodes / NPT);
+    if (local < st.nValid) batch_even_node<St>(st, st.n0 + local);
+  }
 }
 
-void batch_odd_lp(const BatchArgs& a, const BatchLaunch& l, cudaStream_t s) {
-  const size_t smem = 2 * (size_t)kTileAdjBytes;
-  if (a.storage == kStoreF16)
-    k_batch_odd<BStoreF16><<<l.blocks, l.threads, smem, s>>>(a);
+template <class St, int NPT>
+__global__ void __launch_bounds__(kBatchTileNodes / NPT) k_batch_odd_tile(const BatchArgs a) {
+  __shared__ __align__(128) uint32_t sadj[kBatchTileNodes * QM];
+  __shared__ alignas(8) uint64_t bar;
+  __shared__ __align__(16) BatchTile st;
+  if (static_cast<int>(blockIdx.x) >= *a.nTiles) return;
+  if (threadIdx.x < 32) {
+    tile_store(&st, tile_load(a.tiles, blockIdx.x));
+    __syncwarp();
+    if (threadIdx.x == 0) {
+      mbar_init(&bar, 1);
+      mbar_arrive_expect_tx(&bar, kTileAdjBytes);
+      bulk_g2s(sadj, st.adj, kTileAdjBytes, &bar);
+    }
+  }
+  __syncthreads();
+  if (!mbar_wait_bounded(&bar, 0)) {
+    if (threadIdx.x == 0) atomicOr(a.err, 1);
+    return;
+  }
+#pragma unroll 1
+  for (int k = 0; k < NPT; ++k) {
+    const int local = threadIdx.x + k * (kBatchTileNodes / NPT);
+    if (local < st.nValid) batch_odd_node<St>(st, sadj + local * QM, st.n0 + local);
+  }
+}
+
+template <class St>
+static void launch_even(const BatchArgs& a, const BatchLaunch& l, int grid, cudaStream_t s) {
+  if (l.blocks > 0)
+    k_batch_even<St><<<grid, l.threads, 0, s>>>(a);
+  else if (l.nodesPerThread == 4)
+    k_batch_even_tile<St, 4><<<grid, kBatchTileNodes / 4, 0, s>>>(a);
+  else if (l.nodesPerThread == 2)
+    k_batch_even_tile<St, 2><<<grid, kBatchTileNodes / 2, 0, s>>>(a);
   else
-    k_batch_odd<BStoreF32><<<l.blocks, l.threads, smem, s>>>(a);
+    k_batch_even_tile<St, 1><<<grid, kBatchTileNodes, 0, s>>>(a);
+}
+
+template <class St>
+static void launch_odd(const BatchArgs& a, const BatchLaunch& l, int grid, cudaStream_t s) {
+  if (l.blocks > 0)
+    k_batch_odd<St><<<grid, l.threads, 2 * (size_t)kTileAdjBytes, s>>>(a);
+  else if (l.nodesPerThread == 4)
+    k_batch_odd_tile<St, 4><<<grid, kBatchTileNodes / 4, 0, s>>>(a);
+  else if (l.nodesPerThread == 2)
+    k_batch_odd_tile<St, 2><<<grid, kBatchTileNodes / 2, 0, s>>>(a);
+  else
+    k_batch_odd_tile<St, 1><<<grid, kBatchTileNodes, 0, s>>>(a);
+}
+
+void batch_even_lp(const BatchArgs& a, const BatchLaunch& l, int grid, cudaStream_t s) {
+  if (a.storage == kStoreF16)
+    launch_even<BStoreF16>(a, l, grid, s);
+  else
+    launch_even<BStoreF32>(a, l, grid, s);
+}
+
+void batch_odd_lp(const BatchArgs& a, const BatchLaunch& l, int grid, cudaStream_t s) {
+  if (a.storage == kStoreF16)
+    launch_odd<BStoreF16>(a, l, grid, s);
+  else
+    launch_odd<BStoreF32>(a, l, grid, s);
+}
+
+__global__ void k_batch_tiles(const BatchDomain* doms, const int* tileDom, int nTiles, BatchTile* out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nTiles) return;
+  const BatchDomain& D = doms[tileDom[t]];
+  const int lt = t - D.tileStart;
+  BatchTile r;
+  r.adj = D.adj + static_cast<size_t>(lt) * kBatchTileNodes * QM;
+  r.f = D.f;
+  r.nCells = static_cast<int>(D.nCells);
+  r.n0 = lt * kBatchTileNodes;
+  r.nValid = max(0, min(kBatchTileNodes, D.nFluid - r.n0));
+  r.trt = D.trt;
+  out[t] = r;
+}
+
+void batch_build_tiles(const BatchDomain* doms, const int* tileDom, int nTiles, BatchTile* out, cudaStream_t s) {
+  if (nTiles > 0) k_batch_tiles<<<(nTiles + 255) / 256, 256, 0, s>>>(doms, tileDom, nTiles, out);
 }
 
 // ---------------------------------------------------------------------------

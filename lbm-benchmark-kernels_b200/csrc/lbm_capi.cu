@@ -418,20 +418,46 @@ void check_device_error(Gpu* g) {
   }
 }
 
+void vtk_or_exit(LatticeDesc* ld, KernelData* kd, CaseData* cd, int label) {
+  if (lbm_vtk_write(ld, kd, cd, label) != 0) std::exit(1);
+}
+
+// The step loop with VTK output (cd->VtkOutput), as the reference's kernels
+// interleave it (src/BenchKernelD3Q19ListAaPv.c:67-150,
+// src/BenchKernelD3Q19ListPullSplitNt.c:110-254): the state before the first
+// step, after each step pair (AA forms; pull: each step) whose first step
+// index is a multiple of VtkModulus, and after the last step. Each dump
+// synchronises and downloads the mirror; the final dump follows the timed
+// region.
+long enqueue_steps_vtk(LatticeDesc* ld, Gpu* g, CaseData* cd, const lbm::Trt<double>& t) {
+  const int n = cd->MaxIterations, stride = g->kind == kListPull ? 1 : 2;
+  const int modulus = cd->VtkModulus > 0 ? cd->VtkModulus : 1;
+  long k = 0;
+  for (int it = 0; it < n; it += stride) {
+    k += enqueue_steps(g, t, stride);
+    if (it % modulus == 0) {
+      LBM_CK(cudaGetLastError());
+      download(g);
+      vtk_or_exit(ld, &g->kd, cd, it);
+    }
+  }
+  return k;
+}
+
 void cb_kernel(LatticeDesc* ld, KernelData* kd, CaseData* cd) {
-  (void)ld;
   Gpu* g = reinterpret_cast<Gpu*>(kd);
   if (!(cd->Omega > 0.0 && cd->Omega < 2.0)) {
     std::printf("ERROR: omega must lie in (0, 2).\n");
     std::exit(1);
   }
+  if (cd->VtkOutput) vtk_or_exit(ld, kd, cd, -1);
   upload_if_dirty(g);
   const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
 
   LBM_CK(cudaStreamSynchronize(g->stream));
   auto w0 = std::chrono::steady_clock::now();
   LBM_CK(cudaEventRecord(g->ev0, g->stream));
-  g->lastLaunches = enqueue_steps(g, t, cd->MaxIterations);
+  g->lastLaunches = cd->VtkOutput ? enqueue_steps_vtk(ld, g, cd, t) : enqueue_steps(g, t, cd->MaxIterations);
   LBM_CK(cudaGetLastError());
   LBM_CK(cudaEventRecord(g->ev1, g->stream));
   LBM_CK(cudaStreamSynchronize(g->stream));
@@ -442,6 +468,7 @@ void cb_kernel(LatticeDesc* ld, KernelData* kd, CaseData* cd) {
   kd->Duration = std::chrono::duration<double>(w1 - w0).count();
   check_device_error(g);
   download(g);
+  if (cd->VtkOutput) vtk_or_exit(ld, kd, cd, cd->MaxIterations);
 }
 
 // --- Init / Deinit ----------------------------------------------------------------
@@ -573,6 +600,54 @@ void gpu_free(KernelData** kernelData) {
   *kernelData = nullptr;
 }
 
+// --- checkpoints ------------------------------------------------------------------
+
+// FNV-1a (64 bit) of a byte range: the payload check of checkpoint files.
+uint64_t fnv1a64(const void* data, size_t n) {
+  const unsigned char* p = static_cast<const unsigned char*>(data);
+  uint64_t h = 1469598103934665603ull;
+  for (size_t k = 0; k < n; ++k) {
+    h ^= p[k];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+// Instance checkpoint: this header (host byte order), then the current PDF
+// array exactly as the device holds it (storage format, padding included).
+struct CkptHeader {
+  char magic[8];  // "LBMCKPT1"
+  int32_t kind, storage;
+  int32_t dims[3], per[3];
+  int32_t iteration, nFluid;
+  int64_t elems;
+  int32_t elemBytes, reserved;
+  double lambda;
+  uint64_t checksum;
+};
+
+const char kCkptMagic[8] = {'L', 'B', 'M', 'C', 'K', 'P', 'T', '1'};
+
+CkptHeader ckpt_header_of(const Gpu* g) {
+  CkptHeader h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.magic, kCkptMagic, 8);
+  h.kind = (int32_t)g->kind;
+  h.storage = g->storage;
+  for (int i = 0; i < 3; ++i) {
+    h.dims[i] = g->dims[i];
+    h.per[i] = g->per[i];
+  }
+  h.iteration = g->iteration;
+  h.nFluid = g->nFluid;
+  h.elems = (int64_t)g->mirrorElems;
+  h.elemBytes = (int32_t)g->elemBytes;
+  h.lambda = g->lambda;
+  return h;
+}
+
+void* ckpt_payload(Gpu* g) { return g->storage == lbm::kStoreF64 ? static_cast<void*>(g->mirror) : g->rawStage; }
+
 }  // namespace
 
 extern "C" {
@@ -645,6 +720,67 @@ int lbm_b200_sync_mirror(KernelData* kd) {
 }
 
 const char* lbm_b200_last_error(void) { return g_lastError.c_str(); }
+
+int lbm_b200_checkpoint_save(KernelData* kd, const char* path) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (g->dirty) {
+    upload_if_dirty(g);  // the mirror holds SetNode edits: they are the state
+  }
+  cudaError_t e = cudaStreamSynchronize(g->stream);
+  if (e != cudaSuccess) { g_lastError = cudaGetErrorString(e); return (int)e; }
+  download(g);
+  CkptHeader h = ckpt_header_of(g);
+  const size_t bytes = g->mirrorElems * g->elemBytes;
+  h.checksum = fnv1a64(ckpt_payload(g), bytes);
+  FILE* fh = std::fopen(path, "wb");
+  if (!fh) { g_lastError = std::string("cannot open ") + path; return -1; }
+  const bool ok = std::fwrite(&h, sizeof(h), 1, fh) == 1 && std::fwrite(ckpt_payload(g), 1, bytes, fh) == bytes;
+  if (std::fclose(fh) != 0 || !ok) { g_lastError = std::string("writing ") + path + " failed"; return -1; }
+  return 0;
+}
+
+int lbm_b200_checkpoint_load(KernelData* kd, const char* path) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  FILE* fh = std::fopen(path, "rb");
+  if (!fh) { g_lastError = std::string("cannot open ") + path; return -1; }
+  CkptHeader h;
+  const CkptHeader want = ckpt_header_of(g);
+  if (std::fread(&h, sizeof(h), 1, fh) != 1 || std::memcmp(h.magic, kCkptMagic, 8) != 0) {
+    std::fclose(fh);
+    g_lastError = std::string(path) + " is not an instance checkpoint";
+    return -2;
+  }
+  bool same = h.kind == want.kind && h.storage == want.storage && h.nFluid == want.nFluid && h.elems == want.elems &&
+              h.elemBytes == want.elemBytes && h.lambda == want.lambda;
+  for (int i = 0; i < 3; ++i) same = same && h.dims[i] == want.dims[i] && h.per[i] == want.per[i];
+  if (!same) {
+    std::fclose(fh);
+    g_lastError = std::string(path) + " was written by an instance of another kernel, lattice, storage or Lambda";
+    return -2;
+  }
+  cudaError_t e = cudaStreamSynchronize(g->stream);
+  if (e != cudaSuccess) { std::fclose(fh); g_lastError = cudaGetErrorString(e); return (int)e; }
+  const size_t bytes = g->mirrorElems * g->elemBytes;
+  const bool ok = std::fread(ckpt_payload(g), 1, bytes, fh) == bytes;
+  std::fclose(fh);
+  if (!ok) {
+    g_lastError = std::string(path) + " is truncated";
+    download(g);  // the mirror stays the device state
+    return -1;
+  }
+  if (fnv1a64(ckpt_payload(g), bytes) != h.checksum) {
+    g_lastError = std::string(path) + ": checksum mismatch";
+    download(g);  // the mirror stays the device state
+    return -3;
+  }
+  e = cudaMemcpyAsync(current_grid(g), ckpt_payload(g), bytes, cudaMemcpyHostToDevice, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  if (e != cudaSuccess) { g_lastError = cudaGetErrorString(e); return (int)e; }
+  if (g->storage != lbm::kStoreF64) raw_to_mirror(g);
+  g->dirty = false;
+  g->iteration = h.iteration;
+  return 0;
+}
 
 void lbm_b200_mark_mirror_dirty(KernelData* kd) { reinterpret_cast<Gpu*>(kd)->dirty = true; }
 

@@ -45,13 +45,46 @@ struct Trt {
   R force[Q];
 };
 
+// FP32 relaxation constants with the lattice weights as compile-time
+// constants (the same values as a host-built Trt<float>). Per-run data are the
+// two rates and the x body force as its two increments 3 w F_x (w = 1/18,
+// 1/36); force(d) = c_dx times the increment of d's class, which equals the
+// Trt<float> table entry bit for bit. Used where the per-run part sits in
+// shared memory rather than in the kernel's parameter bank.
+struct TrtW {
+  float omegaEven, omegaOdd;
+  float fx1, fx2;
+  __device__ __forceinline__ float force(int d) const {
+    const float v = (d == N || d == S || d == E || d == W || d == T || d == B) ? fx1 : fx2;
+    return cx(d) > 0 ? v : (cx(d) < 0 ? -v : 0.0f);
+  }
+  static constexpr float w0 = static_cast<float>(1.0 / 3.0);
+  static constexpr float w1 = static_cast<float>(1.0 / 18.0);
+  static constexpr float w2 = static_cast<float>(1.0 / 36.0);
+  static constexpr float w1x3 = static_cast<float>(1.0 / 18.0 * 3.0);
+  static constexpr float w2x3 = static_cast<float>(1.0 / 36.0 * 3.0);
+  static constexpr float w1nh = static_cast<float>(1.0 / 18.0 * 9.0 / 2.0);
+  static constexpr float w2nh = static_cast<float>(1.0 / 36.0 * 9.0 / 2.0);
+};
+
+template <class P>
+struct TrtReal;
+template <typename R>
+struct TrtReal<Trt<R>> {
+  using type = R;
+};
+template <>
+struct TrtReal<TrtW> {
+  using type = float;
+};
+
 // One TRT relaxation of a node (src/BenchKernelD3Q19Aa.c:205-284), written as
 // a straight-line function of the 19 incoming PDFs. The operation order is the
 // reference's scalar order; FP64 builds compile this file without FMA
 // contraction, so the results are bit-identical to the reference's scalar
 // kernels. out[i] is the post-collision PDF of direction i (unswapped).
-template <typename R>
-__device__ __forceinline__ void trt_pair(const Trt<R>& t, const R* f, R* out, int a, int b, R ui, R wnh, R wx3,
+template <typename R, class P>
+__device__ __forceinline__ void trt_pair(const P& t, const R* f, R* out, int a, int b, R ui, R wnh, R wx3,
                                          R windep) {
   R evenPart = t.omegaEven * (R(0.5) * (f[a] + f[b]) - ui * ui * wnh - windep);
   R oddPart = t.omegaOdd * (R(0.5) * (f[a] - f[b]) - ui * wx3);
@@ -59,8 +92,8 @@ __device__ __forceinline__ void trt_pair(const Trt<R>& t, const R* f, R* out, in
   out[b] = f[b] - evenPart + oddPart;
 }
 
-template <typename R>
-__device__ __forceinline__ void trt_collide(const Trt<R>& t, const R* f, R* out) {
+template <typename R, class P>
+__device__ __forceinline__ void trt_collide(const P& t, const R* f, R* out) {
   R ux = f[E] + f[NE] + f[SE] + f[TE] + f[BE] - f[W] - f[NW] - f[SW] - f[TW] - f[BW];
   R uy = f[N] + f[NE] + f[NW] + f[TN] + f[BN] - f[S] - f[SE] - f[SW] - f[TS] - f[BS];
   R uz = f[T] + f[TE] + f[TW] + f[TN] + f[TS] - f[B] - f[BE] - f[BW] - f[BN] - f[BS];
@@ -101,8 +134,9 @@ __device__ __forceinline__ P* launder(P* p) {
 // the 19 stores. `load(d)` returns the incoming PDF of direction d,
 // `store(d, v)` writes the post-collision PDF of direction d to its
 // destination.
-template <typename R, class Load, class Store>
-__device__ __forceinline__ void trt_update(const Trt<R>& t, Load load, Store store) {
+template <class P, class Load, class Store>
+__device__ __forceinline__ void trt_update(const P& t, Load load, Store store) {
+  using R = typename TrtReal<P>::type;
   R f[Q], o[Q];
 #pragma unroll
   for (int d = 0; d < Q; ++d) f[d] = load(d);

@@ -14,6 +14,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <strings.h>
+#include <sys/stat.h>
 
 /* D3Q19 velocity set in the reference's order N,S,E,W,NE,SE,NW,SW,T,TN,TE,
  * TW,TS,B,BS,BN,BW,BE,C (src/Kernel.h:121-140): {cx, cy, cz, inverse}. */
@@ -425,6 +426,98 @@ double lbm_verify(LatticeDesc *ld, KernelData *kd, CaseData *cd, int write_file)
 	if (fh) fclose(fh);
 	free(slice);
 	return sqrt(dev);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Legacy VTK dump of one state, the file format of the reference's VtkWrite
+ * (src/Vtk.c:51-245): STRUCTURED_POINTS header, then three binary blocks in
+ * cell order x fastest -- the cell flags as unsigned char, the density
+ * sum_i f_i and the velocity (sum_i c_i f_i, plus F/2 along x: the form of
+ * the reference's VERIFICATION builds, whose body force these kernels always
+ * apply) as big-endian doubles, 0 at obstacles. The sums run in the
+ * reference's order, so an FP64 state that is bit-identical gives a file that
+ * is byte-identical. */
+
+static void vtk_put_be64(FILE *fh, double v)
+{
+	uint64_t u;
+	unsigned char b[8];
+	memcpy(&u, &v, 8);
+	for (int k = 0; k < 8; ++k) b[k] = (unsigned char)(u >> (56 - 8 * k));
+	fwrite(b, 1, 8, fh);
+}
+
+int lbm_vtk_write_file(LatticeDesc *ld, KernelData *kd, CaseData *cd, int iteration, const char *path)
+{
+	const int nx = ld->Dims[0], ny = ld->Dims[1], nz = ld->Dims[2];
+	FILE *fh = fopen(path, "w");
+	if (!fh) return -1;
+	fprintf(fh, "# vtk DataFile Version 1.0\n");
+	fprintf(fh, "Comment: lid driven cavity, iteration % 4d\n", iteration);
+	fprintf(fh, "BINARY\n");
+	fprintf(fh, "DATASET STRUCTURED_POINTS\n");
+	fprintf(fh, "DIMENSIONS %d %d %d\n", nx, ny, nz);
+	fprintf(fh, "ORIGIN 0 0 0 \n");
+	fprintf(fh, "SPACING 1 1 1\n");
+	fprintf(fh, "POINT_DATA %d\n", nx * ny * nz);
+
+	fprintf(fh, "SCALARS NodesTypes unsigned_char 1\n");
+	fprintf(fh, "LOOKUP_TABLE default\n");
+	for (int z = 0; z < nz; ++z) for (int y = 0; y < ny; ++y) for (int x = 0; x < nx; ++x) {
+		unsigned char c = (unsigned char)ld->Lattice[lbmh_lidx(ld->Dims, x, y, z)];
+		fwrite(&c, 1, 1, fh);
+	}
+
+	double p[19];
+	fprintf(fh, "SCALARS Density double\n");
+	fprintf(fh, "LOOKUP_TABLE default\n");
+	for (int z = 0; z < nz; ++z) for (int y = 0; y < ny; ++y) for (int x = 0; x < nx; ++x) {
+		double rho = 0.0;
+		if (ld->Lattice[lbmh_lidx(ld->Dims, x, y, z)] != LAT_CELL_OBSTACLE) {
+			kd->GetNode(kd, x, y, z, p);
+			for (int d = 0; d < 19; ++d) rho += p[d];
+		}
+		vtk_put_be64(fh, rho);
+	}
+
+	fprintf(fh, "VECTORS VelocityVectors double\n");
+	for (int z = 0; z < nz; ++z) for (int y = 0; y < ny; ++y) for (int x = 0; x < nx; ++x) {
+		double ux = 0.0, uy = 0.0, uz = 0.0;
+		if (ld->Lattice[lbmh_lidx(ld->Dims, x, y, z)] != LAT_CELL_OBSTACLE) {
+			kd->GetNode(kd, x, y, z, p);
+			ux = x_velocity(p);
+			uy = p[dN] + p[dNE] + p[dNW] + p[dTN] + p[dBN] - p[dS] - p[dSE] - p[dSW] - p[dTS] - p[dBS];
+			uz = p[dT] + p[dTE] + p[dTW] + p[dTN] + p[dTS] - p[dB] - p[dBE] - p[dBW] - p[dBN] - p[dBS];
+			ux += 0.5 * cd->XForce;
+		}
+		vtk_put_be64(fh, ux);
+		vtk_put_be64(fh, uy);
+		vtk_put_be64(fh, uz);
+	}
+	return fclose(fh) == 0 ? 0 : -1;
+}
+
+int lbm_vtk_write(LatticeDesc *ld, KernelData *kd, CaseData *cd, int iteration)
+{
+	struct stat st;
+	if (stat("vtk", &st) != 0) {
+		if (mkdir("vtk", 0700) != 0) {
+			printf("ERROR: cannot create directory vtk.\n");
+			return -1;
+		}
+		printf("# created directory vtk.\n");
+	} else if (!S_ISDIR(st.st_mode)) {
+		printf("ERROR: cannot create subdirectory vtk as already a file with the same name exists.\n");
+		return -1;
+	}
+	char name[64];
+	snprintf(name, sizeof(name), "vtk/file-%04d.vtk", iteration);
+	printf("# VTK: writing file %s\n", name);
+	if (lbm_vtk_write_file(ld, kd, cd, iteration, name) != 0) {
+		printf("ERROR: writing file %s failed.\n", name);
+		return -1;
+	}
+	return 0;
 }
 
 /* ------------------------------------------------------------------------ */

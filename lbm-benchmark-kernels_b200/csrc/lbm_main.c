@@ -39,7 +39,7 @@ static void usage(void)
 	printf("      [-dims XxYxZ] [-geometry box|channel|pipe|blocks[-value]|fluid|spheres[:seed:porosity:rmin:rmax]]\n");
 	printf("      [-iterations <iterations>] [-rho-in <density>] [-rho-out <density>] [-omega <omega>]\n");
 	printf("      [-x-force <force>] [-kernel <kernel>] [-periodic-x] [-periodic-y] [-periodic-z]\n");
-	printf("      [-verify] [-device <n>] [-t <threads>] [-pin <cores>]\n");
+	printf("      [-verify] [-vtk [<every-n-iteration>]] [-device <n>] [-t <threads>] [-pin <cores>]\n");
 	printf("      -- <kernel specific parameters>\n");
 }
 
@@ -97,7 +97,12 @@ int main(int argc, char *argv[])
 		else if (ARG_IS("-periodic-x")) periodic[0] = 1;
 		else if (ARG_IS("-periodic-y")) periodic[1] = 1;
 		else if (ARG_IS("-periodic-z")) periodic[2] = 1;
-		else if (ARG_IS("-vtk") || ARG_IS("-statistics")) {
+		else if (ARG_IS("-vtk")) {
+			/* src/Main.c:266-285: an optional positive number after the flag is the modulus */
+			cd.VtkOutput = 1;
+			if (i + 1 < argc && atoi(argv[i + 1]) > 0) cd.VtkModulus = atoi(argv[++i]);
+		}
+		else if (ARG_IS("-statistics")) {
 			printf("ERROR: %s is not available in this build.\n", argv[i]);
 			return 1;
 		}

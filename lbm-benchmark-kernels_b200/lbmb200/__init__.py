@@ -156,12 +156,38 @@ def geometry(name, dims, periodic=(0, 0, 0)):
     return lat
 
 
-def case(omega=1.0, xforce=1e-5, iterations=10, rho_in=1.0, rho_out=1.0):
+def case(omega=1.0, xforce=1e-5, iterations=10, rho_in=1.0, rho_out=1.0, vtk=0):
+    """CaseData with the reference's defaults (src/Main.c:140-147); vtk=n > 0
+    asks Kernel for VTK files every n steps (the -vtk n flag)."""
     cd = CaseData()
     cd.Omega, cd.XForce, cd.MaxIterations = omega, xforce, iterations
     cd.RhoIn, cd.RhoOut = rho_in, rho_out
     cd.VtkModulus = cd.StatisticsModulus = 100
+    if vtk:
+        cd.VtkOutput, cd.VtkModulus = 1, int(vtk)
     return cd
+
+
+def write_vtk_field(lattice, field, xforce, iteration, path):
+    """lbm_vtk_write_file on a logical PDF field held on the host (cells x
+    fastest, 19 per cell): the VTK writer of the CUDA rows, fed through a
+    GetNode that reads `field`."""
+    f = np.ascontiguousarray(field, dtype=np.float64).reshape(-1, Q)
+    nx, ny, _ = lattice.dims
+
+    def get_node(_kd, x, y, z, out):
+        row = f[x + nx * (y + ny * z)]
+        for d in range(Q):
+            out[d] = row[d]
+
+    kd = KernelData()
+    cb = _GETNODE(get_node)
+    kd.GetNode = cb
+    cd = case(xforce=xforce)
+    rc = lib().lbm_vtk_write_file(ctypes.byref(lattice.desc), ctypes.byref(kd), ctypes.byref(cd), int(iteration),
+                                  os.fsencode(path))
+    if rc:
+        raise RuntimeError("writing %s failed" % path)
 
 
 class Kernel:
@@ -209,6 +235,25 @@ class Instance:
         """kd->Kernel: cd.MaxIterations steps; returns the kernel's Duration."""
         self.kd.Kernel(ctypes.byref(self.lattice.desc), self.kdp, ctypes.byref(cd))
         return self.kd.Duration
+
+    def write_vtk(self, cd, iteration, path):
+        """lbm_vtk_write_file: the current state as a legacy VTK file."""
+        if lib().lbm_vtk_write_file(ctypes.byref(self.lattice.desc), self.kdp, ctypes.byref(cd), int(iteration),
+                                    os.fsencode(path)):
+            raise RuntimeError("writing %s failed" % path)
+
+    def checkpoint(self, path):
+        """lbm_b200_checkpoint_save: the state, bit for bit, into `path`."""
+        rc = lib().lbm_b200_checkpoint_save(self.kdp, os.fsencode(path))
+        if rc:
+            raise RuntimeError("checkpoint failed (%d): %s" % (rc, lib().lbm_b200_last_error().decode()))
+
+    def restore(self, path):
+        """lbm_b200_checkpoint_load: continue from a checkpoint of an
+        instance of the same kernel, storage, lattice and Lambda."""
+        rc = lib().lbm_b200_checkpoint_load(self.kdp, os.fsencode(path))
+        if rc:
+            raise RuntimeError("restore failed (%d): %s" % (rc, lib().lbm_b200_last_error().decode()))
 
     def step_device(self, cd, n):
         rc = lib().lbm_b200_step_device(self.kdp, ctypes.byref(cd), int(n))
@@ -309,7 +354,7 @@ def _batch_lib():
                      "lbm_batch_sync", "lbm_batch_moments", "lbm_batch_get_field", "lbm_batch_set_field",
                      "lbm_batch_set_launch", "lbm_batch_get_launch", "lbm_batch_time_steps", "lbm_batch_tune",
                      "lbm_batch_bytes_used", "lbm_batch_launches", "lbm_batch_active_domains",
-                     "lbm_batch_fluid_nodes"):
+                     "lbm_batch_fluid_nodes", "lbm_batch_checkpoint_save", "lbm_batch_checkpoint_load"):
             getattr(L, name).argtypes = None
         L.lbm_batch_add.argtypes = [ctypes.c_void_p, ctypes.POINTER(LatticeDesc), ctypes.c_double, ctypes.c_double,
                                     ctypes.c_double]
@@ -371,6 +416,19 @@ class Batch:
         pdfs = np.ascontiguousarray(pdfs, dtype=np.float64).reshape(-1)
         rc = self.L.lbm_batch_set_field(self.h, slot, pdfs.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
         assert rc == 0
+
+    def checkpoint(self, slot, path):
+        """lbm_batch_checkpoint_save: one resident domain, bit for bit."""
+        rc = self.L.lbm_batch_checkpoint_save(self.h, int(slot), os.fsencode(path))
+        if rc:
+            raise RuntimeError("checkpoint failed (%d): %s" % (rc, self.L.lbm_batch_last_error().decode()))
+
+    def restore(self, slot, path):
+        """lbm_batch_checkpoint_load into a slot admitted from the same
+        lattice with the same relaxation parameters."""
+        rc = self.L.lbm_batch_checkpoint_load(self.h, int(slot), os.fsencode(path))
+        if rc:
+            raise RuntimeError("restore failed (%d): %s" % (rc, self.L.lbm_batch_last_error().decode()))
 
     def time_steps(self, n):
         ms = ctypes.c_double(0.0)

@@ -126,6 +126,22 @@ def test_channel_64_lambda_3_16_matches_oracle(oracle):
     assert "%e" % err == "4.915175e+00"
 
 
+@pytest.mark.parametrize("kname", [k[0] for k in KERNELS])
+def test_channel_64_developed_poiseuille_known_answer(kname):
+    # the same channel run to 40000 steps: the developed flow's L2 relative
+    # error against the analytic profile, 1.719602e-02 on the reference build
+    lat = lbmb200.geometry("box", (64, 64, 64), (1, 1, 0))
+    cd = lbmb200.case(omega=1.0, xforce=1.734e-5, iterations=40000)
+    inst = lbmb200.kernel(kname).init(lat, kernel_args=["-lambda", "3/16"])
+    try:
+        inst.set_initial_density(cd)
+        inst.set_initial_velocity(cd)
+        inst.run(cd)
+        assert "%e" % inst.verify(cd) == "1.719602e-02"
+    finally:
+        inst.deinit()
+
+
 def test_list_layout_on_device_instance(oracle):
     lat = lbmb200.geometry("pipe", (10, 12, 11), (0, 0, 0))
     for kname, pull in [("cuda-list-aa-pv-soa", 0), ("cuda-list-pull-split-nt-1s-soa", 1)]:
