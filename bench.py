@@ -174,7 +174,7 @@ def time_kernel(lbmb200, kname, lat, steps, warmup, kargs, dist, odd_key):
             if rc:
                 raise RuntimeError(L.lbm_b200_last_error().decode())
         pairs = (steps + 1) // 2
-        cap = steps if "pull" in kname else 3 * pairs
+        cap = inst.launches_for(steps)
         per = (ctypes.c_double * cap)()
         dist.barrier()
         rc = L.lbm_b200_time_steps(inst.kdp, ctypes.byref(cd), steps, ctypes.byref(tot), per)
@@ -185,7 +185,8 @@ def time_kernel(lbmb200, kname, lat, steps, warmup, kargs, dist, odd_key):
         per = list(per)[:n_launch]
         res = {"ms": tot.value, "launches": n_launch,
                "steps_run": steps if "pull" in kname else 2 * pairs,
-               "per_launch_ms": per, "inst": inst}
+               "per_launch_ms": per, "inst": inst,
+               "launches_per_pair": inst.launches_for(2)}
         return res
     except Exception:
         inst.deinit()
@@ -207,13 +208,14 @@ class _StdoutToStderr:
         os.close(self.saved)
 
 
-def cpu_reference(lat, iterations, threads=None, variant=None):
-    """The reference's list-aa-pv-soa (benchmark build) on this host's cores."""
+def cpu_reference(lat, iterations, threads=None, variant=None, kernel="list-aa-pv-soa"):
+    """A reference kernel (benchmark build; list-aa-pv-soa by default) on this
+    host's cores."""
     with _StdoutToStderr():
-        return _cpu_reference(lat, iterations, threads, variant)
+        return _cpu_reference(lat, iterations, threads, variant, kernel)
 
 
-def _cpu_reference(lat, iterations, threads=None, variant=None):
+def _cpu_reference(lat, iterations, threads=None, variant=None, kernel="list-aa-pv-soa"):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import Reference, reference_available
     if variant is None:
@@ -223,12 +225,40 @@ def _cpu_reference(lat, iterations, threads=None, variant=None):
         return None
     ref = Reference(variant)
     threads = ref.set_threads(threads or os.cpu_count() or 1)
-    ref.run("list-aa-pv-soa", lat.dims, lat.periodic, lat.mask, omega=1.0, xforce=1e-5,
+    ref.run(kernel, lat.dims, lat.periodic, lat.mask, omega=1.0, xforce=1e-5,
             iterations=iterations, init="zero", want_pdfs=False)
     dur = ref.last_duration
     it = iterations + (iterations % 2)  # the AA loop runs whole pairs
     return {"mflups": lat.n_fluid * it / dur / 1e6, "seconds": dur, "iterations": it, "threads": threads,
             "variant": variant}
+
+
+def aa_line(lbmb200, fl, args, kargs, dist, peak):
+    """Device-timed cuda-aa-soa steps on lattice `fl`: MFLUP/s, HBM fraction,
+    per-launch split of each even/odd pair, and the reference's fastest
+    full-array CPU kernel (aa-vec-soa) on the same lattice beside it."""
+    ta = time_kernel(lbmb200, "cuda-aa-soa", fl, min(args.steps, 200), 4, kargs, dist, "aa")
+    ta["inst"].deinit()
+    per, lpp = ta["per_launch_ms"], ta["launches_per_pair"]
+    # per pair: even step, then the odd step's launches (interior blocks without
+    # and with reversed links, face shell)
+    pairs = [per[k:k + lpp] for k in range(0, len(per) - lpp + 1, lpp)]
+    ev = statistics.mean(p[0] for p in pairs)
+    od = statistics.mean(sum(p[1:]) for p in pairs)
+    am = (ev + od) / 2
+    out = {"fluid_nodes": fl.n_fluid, "mflups": round(fl.n_fluid / (am / 1e3) / 1e6, 1),
+           "achieved_gbs": round(B_PER_FLUP["aa"] * fl.n_fluid / (am / 1e3) / 1e9, 1),
+           "frac": round(B_PER_FLUP["aa"] * fl.n_fluid / (am / 1e3) / 1e9 / peak, 4),
+           "even_ms": round(ev, 5), "odd_ms": round(od, 5),
+           "odd_launch_ms": [round(statistics.mean(p[k] for p in pairs), 5) for k in range(1, lpp)]}
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
+        probe = cpu_reference(fl, 2, kernel="aa-vec-soa")
+        if probe is not None:
+            iters = int(max(2, min(200, 5.0 * probe["mflups"] * 1e6 / fl.n_fluid)))
+            r = cpu_reference(fl, iters + iters % 2, kernel="aa-vec-soa")
+            out["cpu_reference"] = {"mflups": round(r["mflups"], 1), "cores": r["threads"],
+                                    "sample": "%d steps, reference aa-vec-soa (%s build)" % (r["iterations"], r["variant"])}
+    return out
 
 
 def cpu_model():
@@ -460,22 +490,13 @@ def run_ours(args, dist):
             "mflups": round(lat.n_fluid / (pm / 1e3) / 1e6, 1), "launch_ms": round(pm, 5),
             "achieved_gbs": round(B_PER_FLUP["pull"] * lat.n_fluid / (pm / 1e3) / 1e9, 1),
             "frac": round(B_PER_FLUP["pull"] * lat.n_fluid / (pm / 1e3) / 1e9 / peak, 4)}
-        # full-array AA on a fully periodic 256^3 box (the reference's -geometry fluid with
-        # -periodic-x -periodic-y -periodic-z)
-        fl = lbmb200.geometry("fluid", (args.edge,) * 3, (1, 1, 1))
-        ta = time_kernel(lbmb200, "cuda-aa-soa", fl, min(args.steps, 200), 4, kargs, dist, "aa")
-        ta["inst"].deinit()
-        per = ta["per_launch_ms"]  # per pair: even, odd interior, odd face shell
-        ev = statistics.mean(per[0::3])
-        od = statistics.mean([a + b for a, b in zip(per[1::3], per[2::3])])
-        am = (ev + od) / 2
-        extra["cuda-aa-soa"] = {
-            "workload": "%d^3 fully periodic fluid box" % args.edge, "fluid_nodes": fl.n_fluid,
-            "mflups": round(fl.n_fluid / (am / 1e3) / 1e6, 1),
-            "achieved_gbs": round(B_PER_FLUP["aa"] * fl.n_fluid / (am / 1e3) / 1e9, 1),
-            "frac": round(B_PER_FLUP["aa"] * fl.n_fluid / (am / 1e3) / 1e9 / peak, 4),
-            "even_ms": round(ev, 5), "odd_ms": round(od, 5),
-            "odd_face_ms": round(statistics.mean(per[2::3]), 5)}
+        # full-array AA at 256^3: the reference's -geometry fluid with -periodic-x -periodic-y
+        # -periodic-z, and -geometry channel (x periodic, walls in y and z)
+        for key, geo, per_flags in (("cuda-aa-soa", "fluid", (1, 1, 1)), ("cuda-aa-soa/channel", "channel", (0, 0, 0))):
+            fl = lbmb200.geometry(geo, (args.edge,) * 3, per_flags)
+            extra[key] = aa_line(lbmb200, fl, args, kargs, dist, peak)
+            extra[key]["workload"] = "%d^3 %s" % (args.edge, "fully periodic fluid box" if geo == "fluid"
+                                                  else "channel, periodic x, walls in y and z")
         # reduced storage list AA on the porous domain (FP32 arithmetic)
         for prec, pb in (("fp32", 4), ("fp16", 2)):
             tl = time_kernel(lbmb200, "cuda-list-aa-pv-soa", lat, min(args.steps, 200), 4,

@@ -216,6 +216,12 @@ void lbm_b200_mark_mirror_dirty(KernelData *kd);
  * error code. */
 int lbm_b200_time_steps(KernelData *kd, CaseData *cd, int n, double *total_ms, double *per_launch_ms);
 
+/* Number of kernel launches that n time steps take on this instance (the
+ * size of lbm_b200_time_steps' per_launch_ms): AA kernels run whole even/odd
+ * pairs of 2-4 launches (even step; odd step interior blocks without and with
+ * reversed links; face shell), list AA 2 per pair, pull 1 per step. */
+long lbm_b200_launches_for(KernelData *kd, int n);
+
 /* Runs a kernel that waits, with a bound of `polls` reads, on a device flag
  * that nothing sets: the wait runs out, the kernel records error bit 2 in its
  * error word and returns, and *status receives the word (2). The same bounded

@@ -337,17 +337,8 @@ int lbm_batch_reset(void* h, int slot) {
   Batch* b = static_cast<Batch*>(h);
   DomainSlot& d = b->slots[slot];
   const size_t nc = (size_t)d.dev.nCells;
-  if (b->storage == lbm::kStoreF16) {
-    BCK(cudaMemsetAsync(d.pdfs, 0, nc * Q * 2, b->stream));
-  } else {
-    std::vector<float> plane(nc);
-    for (int q = 0; q < Q; ++q) {
-      std::fill(plane.begin(), plane.end(), (float)weight_of(q));
-      BCK(cudaMemcpyAsync(static_cast<float*>(d.pdfs) + q * nc, plane.data(), nc * 4, cudaMemcpyHostToDevice,
-                          b->stream));
-      BCK(cudaStreamSynchronize(b->stream));
-    }
-  }
+  // both storage formats hold deviations from w: rest is all zero bits
+  BCK(cudaMemsetAsync(d.pdfs, 0, nc * Q * b->elemBytes, b->stream));
   return 0;
 }
 
@@ -423,7 +414,7 @@ int lbm_batch_get_field(void* h, int slot, double* out) {
       const size_t k = (size_t)q * nc + n;
       double v;
       if (b->storage == lbm::kStoreF32)
-        v = (double)reinterpret_cast<const float*>(raw.data())[k];
+        v = weight_of(q) + (double)reinterpret_cast<const float*>(raw.data())[k];
       else
         v = weight_of(q) + (double)lbmh_f16_to_f32(reinterpret_cast<const uint16_t*>(raw.data())[k]) / f16_scale_of(q);
       out[c * Q + q] = v;
@@ -447,7 +438,7 @@ int lbm_batch_set_field(void* h, int slot, const double* in) {
     for (int q = 0; q < Q; ++q) {
       const size_t k = (size_t)q * nc + n;
       if (b->storage == lbm::kStoreF32)
-        reinterpret_cast<float*>(raw.data())[k] = (float)in[c * Q + q];
+        reinterpret_cast<float*>(raw.data())[k] = (float)(in[c * Q + q] - weight_of(q));
       else
         reinterpret_cast<uint16_t*>(raw.data())[k] =
             lbmh_f32_to_f16((float)((in[c * Q + q] - weight_of(q)) * f16_scale_of(q)));

@@ -6,29 +6,11 @@
 // (256 nodes x 18 entries, 18 KB, contiguous) into shared memory with one
 // bulk copy, double buffered: while a tile is relaxed, the bulk copy of the
 // block's next tile is already in flight.
-#include <cuda_fp16.h>
-
 #include "lbm_batch.cuh"
 #include "lbm_bulk.cuh"
+#include "lbm_store.cuh"
 
 namespace lbm {
-
-__device__ __forceinline__ float bweight(int d) {
-  return d == DC ? 1.0f / 3.0f : (d == N || d == S || d == E || d == W || d == T || d == B) ? 1.0f / 18.0f : 1.0f / 36.0f;
-}
-
-struct BStoreF32 {
-  using T = float;
-  __device__ static float dev(T raw, int d) { return raw - bweight(d); }
-  __device__ static T raw(float delta, int d) { return bweight(d) + delta; }
-};
-
-struct BStoreF16 {
-  using T = __half;
-  __device__ static float scale(int d) { return d == DC ? 32768.0f : (bweight(d) > 0.05f ? 262144.0f : 524288.0f); }
-  __device__ static float dev(T raw, int d) { return __half2float(raw) * (1.0f / scale(d)); }
-  __device__ static T raw(float delta, int d) { return __float2half_rn(delta * scale(d)); }
-};
 
 // Warp 0 moves tile records: each lane loads one 32-bit word (the load of the
 // block's next-but-one record is issued before the current tile is updated
@@ -230,16 +212,16 @@ static void launch_odd(const BatchArgs& a, const BatchLaunch& l, int grid, cudaS
 
 void batch_even_lp(const BatchArgs& a, const BatchLaunch& l, int grid, cudaStream_t s) {
   if (a.storage == kStoreF16)
-    launch_even<BStoreF16>(a, l, grid, s);
+    launch_even<StoreF16>(a, l, grid, s);
   else
-    launch_even<BStoreF32>(a, l, grid, s);
+    launch_even<StoreF32>(a, l, grid, s);
 }
 
 void batch_odd_lp(const BatchArgs& a, const BatchLaunch& l, int grid, cudaStream_t s) {
   if (a.storage == kStoreF16)
-    launch_odd<BStoreF16>(a, l, grid, s);
+    launch_odd<StoreF16>(a, l, grid, s);
   else
-    launch_odd<BStoreF32>(a, l, grid, s);
+    launch_odd<StoreF32>(a, l, grid, s);
 }
 
 __global__ void k_batch_tiles(const BatchDomain* doms, const int* tileDom, int nTiles, BatchTile* out) {
@@ -322,9 +304,9 @@ void batch_moments(const BatchArgs& a, int maxTiles, double* tilePartials, const
                    const int* domTileCount, int nDomSlots, double* out, cudaStream_t s) {
   const int blocks = maxTiles < 4096 ? (maxTiles > 0 ? maxTiles : 1) : 4096;
   if (a.storage == kStoreF16)
-    k_batch_moments_tile<BStoreF16><<<blocks, kBatchTileNodes, 0, s>>>(a, maxTiles, tilePartials);
+    k_batch_moments_tile<StoreF16><<<blocks, kBatchTileNodes, 0, s>>>(a, maxTiles, tilePartials);
   else
-    k_batch_moments_tile<BStoreF32><<<blocks, kBatchTileNodes, 0, s>>>(a, maxTiles, tilePartials);
+    k_batch_moments_tile<StoreF32><<<blocks, kBatchTileNodes, 0, s>>>(a, maxTiles, tilePartials);
   k_batch_moments_dom<<<(nDomSlots + 127) / 128, 128, 0, s>>>(tilePartials, domTileStart, domTileCount, nDomSlots, out);
 }
 

@@ -59,6 +59,8 @@ struct Gpu {
   // AA layout
   int xs, pitch;
   long long dstride;
+  int* dOddBlocks;         // interior blocks of the odd step: nDirect direct, then nGeneral general
+  int nDirect, nGeneral;
 
   // list layout
   uint32_t* grid;
@@ -292,14 +294,19 @@ long enqueue_steps(Gpu* g, const lbm::Trt<double>& t, int n, cudaEvent_t* ev = n
   };
   if (g->kind == kAa) {
     lbm::AaArgs a = aa_args(g);
-    const bool interior = lbm::aa_has_interior(a), shell = lbm::aa_shell_cells(a) > 0;
+    const bool shell = lbm::aa_shell_cells(a) > 0;
     for (int it = 0; it < n; it += 2) {
       mark();
       lbm::aa_even_fp64(a, t, g->stream);
       ++k;
-      if (interior) {
+      if (g->nDirect > 0) {
         mark();
-        lbm::aa_odd_interior_fp64(a, t, g->stream);
+        lbm::aa_odd_interior_fp64(a, t, g->dOddBlocks, g->nDirect, 0, g->stream);
+        ++k;
+      }
+      if (g->nGeneral > 0) {
+        mark();
+        lbm::aa_odd_interior_fp64(a, t, g->dOddBlocks + g->nDirect, 0, g->nGeneral, g->stream);
         ++k;
       }
       if (shell) {
@@ -351,7 +358,7 @@ long launches_for(Gpu* g, int n) {
   long perPair = 2;
   if (g->kind == kAa) {
     const lbm::AaArgs a = aa_args(g);
-    perPair = 1 + (lbm::aa_has_interior(a) ? 1 : 0) + (lbm::aa_shell_cells(a) > 0 ? 1 : 0);
+    perPair = 1 + (g->nDirect > 0) + (g->nGeneral > 0) + (lbm::aa_shell_cells(a) > 0 ? 1 : 0);
   }
   return perPair * ((n + 1) / 2);
 }
@@ -362,7 +369,7 @@ void mirror_to_raw(Gpu* g) {
   const size_t n = g->mirrorElems, nc = (size_t)g->nCells;
   if (g->storage == lbm::kStoreF32) {
     float* r = static_cast<float*>(g->rawStage);
-    for (size_t k = 0; k < n; ++k) r[k] = (float)g->mirror[k];
+    for (size_t k = 0; k < n; ++k) r[k] = (float)(g->mirror[k] - weight_of((int)(k / nc)));
   } else {
     uint16_t* r = static_cast<uint16_t*>(g->rawStage);
     for (size_t k = 0; k < n; ++k) {
@@ -376,7 +383,7 @@ void raw_to_mirror(Gpu* g) {
   const size_t n = g->mirrorElems, nc = (size_t)g->nCells;
   if (g->storage == lbm::kStoreF32) {
     const float* r = static_cast<const float*>(g->rawStage);
-    for (size_t k = 0; k < n; ++k) g->mirror[k] = (double)r[k];
+    for (size_t k = 0; k < n; ++k) g->mirror[k] = weight_of((int)(k / nc)) + (double)r[k];
   } else {
     const uint16_t* r = static_cast<const uint16_t*>(g->rawStage);
     for (size_t k = 0; k < n; ++k) {
@@ -529,9 +536,23 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params) {
     lbmh_aa_links(ld, g->xs, g->pitch, lbm::kZOff, link);
     LBM_CK(cudaMalloc(&g->dLink, sizeof(uint32_t) * (size_t)g->dstride));
     LBM_CK(cudaMemcpy(g->dLink, link, sizeof(uint32_t) * (size_t)g->dstride, cudaMemcpyHostToDevice));
-    std::free(link);
     LBM_CK(cudaMalloc(&g->dF, sizeof(double) * g->mirrorElems));
     LBM_CK(cudaMemset(g->dF, 0, sizeof(double) * g->mirrorElems));
+    // the odd step's interior blocks, direct ones first
+    const lbm::AaArgs aa = aa_args(g);
+    const long long nb = lbm::aa_interior_block_count(aa);
+    if (nb > 0) {
+      int* blocks = static_cast<int*>(std::malloc(sizeof(int) * (size_t)nb));
+      if (!blocks) { std::printf("ERROR: allocation failed.\n"); std::exit(1); }
+      lbm::aa_interior_blocks(aa, link, blocks, &g->nDirect, &g->nGeneral);
+      if (g->nDirect + g->nGeneral > 0) {
+        LBM_CK(cudaMalloc(&g->dOddBlocks, sizeof(int) * (size_t)(g->nDirect + g->nGeneral)));
+        LBM_CK(cudaMemcpy(g->dOddBlocks, blocks, sizeof(int) * (size_t)(g->nDirect + g->nGeneral),
+                          cudaMemcpyHostToDevice));
+      }
+      std::free(blocks);
+    }
+    std::free(link);
   } else {
     const bool pull = kind == kListPull;
     int nCells = lbmh_pad_cells(ld->nFluid, (int)sizeof(double), a.pad);
@@ -586,6 +607,7 @@ void gpu_free(KernelData** kernelData) {
   cudaFree(g->dF);
   cudaFree(g->dG);
   cudaFree(g->dLink);
+  cudaFree(g->dOddBlocks);
   cudaFree(g->dAdj);
   cudaFree(g->dErr);
   cudaFree(g->dMomOut);
@@ -720,6 +742,8 @@ int lbm_b200_sync_mirror(KernelData* kd) {
 }
 
 const char* lbm_b200_last_error(void) { return g_lastError.c_str(); }
+
+long lbm_b200_launches_for(KernelData* kd, int n) { return launches_for(reinterpret_cast<Gpu*>(kd), n); }
 
 int lbm_b200_checkpoint_save(KernelData* kd, const char* path) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);

@@ -26,6 +26,7 @@ namespace lbm {
 // (a wall: bounce back, or an open non-periodic face).
 constexpr int kZOff = 4;
 constexpr uint32_t kFluidBit = 0x80000000u;
+constexpr uint32_t kLinkBits = 0x3ffffu;  // the 18 reversed-link bits
 
 struct AaArgs {
   double* f;
@@ -74,8 +75,17 @@ struct ListArgsLp {
 void list_even_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s);
 void list_odd_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s);
 void aa_even_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
-// The AA odd step is two launches: the interior cells, then the face shell.
-void aa_odd_interior_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
+// The AA odd step: the interior blocks (a list of nDirect blocks for the
+// direct kernel, followed by nGeneral blocks for the general one, built by
+// aa_interior_blocks), then the face shell.
+void aa_odd_interior_fp64(const AaArgs& a, const Trt<double>& t, const int* blocks, int nDirect, int nGeneral,
+                          cudaStream_t s);
+// Host: sorts the interior blocks of the odd step by the link words of their
+// cells (link: the host copy of the device link array). Fills `blocks` (room
+// for aa_interior_block_count entries) with the direct blocks, then the
+// general ones; blocks without fluid cells are left out.
+long long aa_interior_block_count(const AaArgs& a);
+void aa_interior_blocks(const AaArgs& a, const uint32_t* link, int* blocks, int* nDirect, int* nGeneral);
 void aa_odd_face_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
 bool aa_has_interior(const AaArgs& a);
 long long aa_shell_cells(const AaArgs& a);

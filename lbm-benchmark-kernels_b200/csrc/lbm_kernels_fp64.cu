@@ -22,6 +22,8 @@
 // its odd step and then overwrites what they wrote with the fix-up lists
 // (src/BenchKernelD3Q19Aa.c:301-311,501-511); here periodic wraps and bounce
 // back are resolved at the load/store itself, so no fix-up pass exists.
+#include <vector>
+
 #include "lbm_bulk.cuh"
 #include "lbm_kernels.cuh"
 
@@ -79,19 +81,38 @@ __global__ void __launch_bounds__(128) k_aa_even_fp64(const AaArgs a, const Trt<
 // (x + c_i, i) with the increment of i, or -- bounced back at a wall -- to
 // its own slot (x, inv(i)) with the increment of inv(i).
 //
-// Two kernels share the step. The interior kernel takes every cell off the x
-// and y faces -- and off the z faces too unless z is periodic: links of these
-// cells leave the domain at most through a periodic z face, which is a fixed
-// offset of -/+ nZ cells, so each address is a select between the
-// neighbour's slot and the node's own slot and the 19 loads are issued
+// Three launches share the step. The interior kernels take every cell off
+// the x and y faces -- and off the z faces too unless z is periodic: links of
+// these cells leave the domain at most through a periodic z face, which is a
+// fixed offset of -/+ nZ cells. Their blocks (32 z-cells x 4 y-rows of one x
+// plane) are sorted on the host into two lists: blocks whose fluid cells have
+// no reversed link run the direct kernel, where every address is the
+// neighbour's slot; the others run the general kernel, where each address is
+// a select between the neighbour's slot and the node's own slot. Blocks
+// without fluid cells are not launched. In both, the 19 loads are issued
 // together. The face kernel takes the remaining shell: links that leave the
 // domain wrap periodically on every crossed axis, or, at a non-periodic face,
 // go to the ghost layer (an "open" link), as in the reference.
-__global__ void __launch_bounds__(128) k_aa_odd_interior_fp64(const AaArgs a, const Trt<double> t) {
-  const int zLo = a.perZ ? 0 : 1, zHi = a.perZ ? a.nZ - 1 : a.nZ - 2;
-  const int z = zLo + blockIdx.x * 32 + threadIdx.x;
-  const int y = 1 + blockIdx.y * 4 + threadIdx.y;
-  const int x = 1 + blockIdx.z;
+//
+// Cells of different nodes never share a slot in the odd step (each node
+// reads and writes only its own links' slots), so the three launches may run
+// in any order.
+
+// Interior block `id` of the list: (bz, by, bx) with bz fastest.
+__device__ __forceinline__ void aa_interior_block(const AaArgs& a, int id, int& z, int& y, int& x) {
+  const int nz = a.perZ ? a.nZ : a.nZ - 2;
+  const int gz = (nz + 31) / 32, gy = (a.nY - 2 + 3) / 4;
+  const int bz = id % gz, rest = id / gz;
+  z = (a.perZ ? 0 : 1) + bz * 32 + threadIdx.x;
+  y = 1 + (rest % gy) * 4 + threadIdx.y;
+  x = 1 + rest / gy;
+}
+
+template <bool kDirect>
+__global__ void __launch_bounds__(128) k_aa_odd_interior_fp64(const AaArgs a, const Trt<double> t, const int* blocks) {
+  int x, y, z;
+  aa_interior_block(a, blocks[blockIdx.x], z, y, x);
+  const int zHi = a.perZ ? a.nZ - 1 : a.nZ - 2;
   if (z > zHi || y > a.nY - 2) return;
   const int c = aa_cell(a, x, y, z);
   const uint32_t w = __ldg(a.link + c);
@@ -102,14 +123,20 @@ __global__ void __launch_bounds__(128) k_aa_odd_interior_fp64(const AaArgs a, co
   auto nbr = [&](int d) -> int {
     return c + aa_off(a, d) + (cz(d) < 0 ? wrapDown : (cz(d) > 0 ? wrapUp : 0));
   };
+  if (kDirect) {
+    // store addresses come from laundered plane pointers, apart from the load
+    // addresses, so those need not stay live across the collision
+    trt_update(
+        t, [&](int d) -> double { return a.plane[inv(d)][d == DC ? c : nbr(inv(d))] + t.force[d]; },
+        [&](int d, double v) { launder(a.plane[d])[d == DC ? c : nbr(d)] = v + t.force[d]; });
+    return;
+  }
   auto load = [&](int d) -> double {
     if (d == DC) return a.plane[DC][c] + t.force[DC];
     const int j = inv(d);
     const bool rev = (w >> j) & 1u;
     return (rev ? a.plane[d] + c : a.plane[j] + nbr(j))[0] + t.force[d];
   };
-  // store addresses are formed from laundered plane pointers, apart from the
-  // load addresses, so those need not stay live across the collision
   auto store = [&](int d, double v) {
     if (d == DC) {
       launder(a.plane[DC])[c] = v + t.force[DC];
@@ -197,16 +224,53 @@ long long aa_shell_cells(const AaArgs& a) {
 
 bool aa_has_interior(const AaArgs& a) { return a.nX > 2 && a.nY > 2 && (a.perZ || a.nZ > 2); }
 
+long long aa_interior_block_count(const AaArgs& a) {
+  if (!aa_has_interior(a)) return 0;
+  const long long nz = a.perZ ? a.nZ : a.nZ - 2;
+  return (nz + 31) / 32 * ((a.nY - 2 + 3) / 4) * (long long)(a.nX - 2);
+}
+
+void aa_interior_blocks(const AaArgs& a, const uint32_t* link, int* blocks, int* nDirect, int* nGeneral) {
+  *nDirect = *nGeneral = 0;
+  const long long n = aa_interior_block_count(a);
+  if (n == 0) return;
+  const int zLo = a.perZ ? 0 : 1, zHi = a.perZ ? a.nZ - 1 : a.nZ - 2;
+  const int gz = (zHi - zLo + 1 + 31) / 32, gy = (a.nY - 2 + 3) / 4;
+  std::vector<int> general;
+  for (long long id = 0; id < n; ++id) {
+    const int bz = (int)(id % gz), by = (int)(id / gz % gy), bx = (int)(id / gz / gy);
+    bool fluid = false, reversed = false;
+    for (int ty = 0; ty < 4; ++ty) {
+      const int y = 1 + by * 4 + ty;
+      if (y > a.nY - 2) break;
+      for (int tz = 0; tz < 32; ++tz) {
+        const int z = zLo + bz * 32 + tz;
+        if (z > zHi) break;
+        const uint32_t w = link[(long long)(bx + 2) * a.xs + (long long)(y + 1) * a.pitch + z + kZOff];
+        if (!(w & kFluidBit)) continue;
+        fluid = true;
+        reversed = reversed || (w & kLinkBits) != 0;
+      }
+    }
+    if (!fluid) continue;
+    if (reversed)
+      general.push_back((int)id);
+    else
+      blocks[(*nDirect)++] = (int)id;
+  }
+  for (int id : general) blocks[*nDirect + (*nGeneral)++] = id;
+}
+
 static dim3 aa_grid(const AaArgs& a) { return dim3((a.nZ + 31) / 32, (a.nY + 3) / 4, a.nX); }
 
 void aa_even_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
   k_aa_even_fp64<<<aa_grid(a), dim3(32, 4), 0, s>>>(a, t);
 }
 
-void aa_odd_interior_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
-  if (!aa_has_interior(a)) return;
-  const int nz = a.perZ ? a.nZ : a.nZ - 2;
-  k_aa_odd_interior_fp64<<<dim3((nz + 31) / 32, (a.nY - 2 + 3) / 4, a.nX - 2), dim3(32, 4), 0, s>>>(a, t);
+void aa_odd_interior_fp64(const AaArgs& a, const Trt<double>& t, const int* blocks, int nDirect, int nGeneral,
+                          cudaStream_t s) {
+  if (nDirect > 0) k_aa_odd_interior_fp64<true><<<nDirect, dim3(32, 4), 0, s>>>(a, t, blocks);
+  if (nGeneral > 0) k_aa_odd_interior_fp64<false><<<nGeneral, dim3(32, 4), 0, s>>>(a, t, blocks + nDirect);
 }
 
 void aa_odd_face_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {

@@ -1,41 +1,12 @@
 // lbm_kernels_lp.cu -- reduced-storage list AA kernels for sm_100a: PDFs kept
-// in HBM as FP32, or as FP16 deviations from the lattice weights, with the
-// collision evaluated in FP32 (FMA contraction allowed in this file).
-//
-// Deviation form. With f_i = w_i + delta_i, the TRT update of
-// lbm_d3q19.cuh holds unchanged for the deltas once "dens" is replaced by
-// sum_i delta_i (= rho - 1): the momentum sum_i c_i w_i vanishes and the
-// weight terms cancel in both parts of each pair. Working on deltas keeps the
-// O(1) background out of the FP32 arithmetic.
-//
-// Storage:
-//   StoreF32  raw = w_i + delta_i as float (delta = raw - w_i is exact while
-//             raw stays within a factor 2 of w_i)
-//   StoreF16  raw = half(delta_i * 2^k_i), k_i fixed per direction class
-//             (k = 15, 18, 19 for w = 1/3, 1/18, 1/36), so that |delta| up to
-//             ~4.5 w_i is representable and deltas down to ~2e-10 stay normal.
+// in HBM as FP32 or FP16 deviations from the lattice weights (lbm_store.cuh),
+// with the collision evaluated in FP32 (FMA contraction allowed in this file).
 // Bytes per fluid-lattice update: even 19*2*s, odd 19*2*s + 72 (s = 4 or 2).
-#include <cuda_fp16.h>
-
 #include "lbm_bulk.cuh"
 #include "lbm_kernels.cuh"
+#include "lbm_store.cuh"
 
 namespace lbm {
-
-__device__ __forceinline__ float weight_f(int d) { return d == DC ? 1.0f / 3.0f : (d == N || d == S || d == E || d == W || d == T || d == B) ? 1.0f / 18.0f : 1.0f / 36.0f; }
-
-struct StoreF32 {
-  using T = float;
-  __device__ static float dev(T raw, int d) { return raw - weight_f(d); }
-  __device__ static T raw(float delta, int d) { return weight_f(d) + delta; }
-};
-
-struct StoreF16 {
-  using T = __half;
-  __device__ static float scale(int d) { return d == DC ? 32768.0f : (weight_f(d) > 0.05f ? 262144.0f : 524288.0f); }
-  __device__ static float dev(T raw, int d) { return __half2float(raw) * (1.0f / scale(d)); }
-  __device__ static T raw(float delta, int d) { return __float2half_rn(delta * scale(d)); }
-};
 
 template <class St>
 __global__ void __launch_bounds__(kListTile) k_list_even_lp(const ListArgsLp a, const Trt<float> t) {
@@ -83,7 +54,7 @@ __global__ void __launch_bounds__(kListTile) k_list_odd_lp(const ListArgsLp a, c
     const uint32_t dst = reinterpret_cast<const volatile uint32_t*>(e)[d];  // re-read: keeps no 64-bit addresses live across the collision
     const int j = inv(d);
     const bool bounce = dst == static_cast<uint32_t>(j * S + n);
-    f[dst] = St::raw(v + (bounce ? t.force[j] : t.force[d]), d);  // w and the scale are equal for d and inv(d)
+    f[dst] = St::raw(v + (bounce ? t.force[j] : t.force[d]), d);  // the scale is equal for d and inv(d)
   };
   trt_update(t, load, store);
 }

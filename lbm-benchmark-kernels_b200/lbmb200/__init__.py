@@ -95,6 +95,7 @@ def lib():
         L.lbm_b200_kernels.argtypes = [ctypes.POINTER(ctypes.c_int)]
         L.lbm_b200_last_device_ms.restype = ctypes.c_double
         L.lbm_b200_last_launches.restype = ctypes.c_long
+        L.lbm_b200_launches_for.restype = ctypes.c_long
         L.lbm_b200_last_error.restype = ctypes.c_char_p
         L.lbm_verify.restype = ctypes.c_double
         L.lbm_density.restype = ctypes.c_double
@@ -235,6 +236,10 @@ class Instance:
         """kd->Kernel: cd.MaxIterations steps; returns the kernel's Duration."""
         self.kd.Kernel(ctypes.byref(self.lattice.desc), self.kdp, ctypes.byref(cd))
         return self.kd.Duration
+
+    def launches_for(self, n):
+        """Kernel launches that n time steps take on this instance."""
+        return int(lib().lbm_b200_launches_for(self.kdp, int(n)))
 
     def write_vtk(self, cd, iteration, path):
         """lbm_vtk_write_file: the current state as a legacy VTK file."""
