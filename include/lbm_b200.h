@@ -298,6 +298,15 @@ int lbmh_pad_cells(int nCells, int pdfBytes, const char *padStr);
 int lbmh_list_build(const LatticeDesc *ld, int pull, const int blk[3], int nCells,
                     uint32_t *grid, uint32_t *coords, uint32_t *adj);
 
+/* The same layout built on the GPU (what the list rows' Init and
+ * lbm_batch_add use): numbering in the blocked order by a prefix sum over the
+ * cells, then each node's 18 links; host mask in, host grid (nX*nY*nZ) and
+ * adjacency (ld->nFluid*18) out, bit-identical to lbmh_list_build. Returns
+ * the fluid node count, -1 on a CUDA error, -2 when the mask holds more
+ * non-obstacle cells than ld->nFluid (nothing written to adj). */
+int lbm_b200_list_build(const LatticeDesc *ld, int pull, const int blk[3], int nCells, uint32_t *grid,
+                        uint32_t *adj);
+
 /* ---- Batched domains (no counterpart in the reference) ----
  * Many independent porous domains of uneven size, each with its own list
  * layout (push adjacency as the list AA kernel, node range padded to tiles of

@@ -290,17 +290,33 @@ int lbm_batch_add(void* h, const LatticeDesc* ld, double omega, double lambda, d
   d = DomainSlot();
   const long ncell = (long)ld->Dims[0] * ld->Dims[1] * ld->Dims[2];
   d.grid.resize(ncell);
-  std::vector<uint32_t> adj((size_t)nCells * QM, 0u);
-  const int blk[3] = {0, 0, 0};
-  const int nf = lbmh_list_build(ld, 0, blk, (int)nCells, d.grid.data(), nullptr, adj.data());
-  if (nf != nFluid) return -6;
-  // padding nodes point at their own slots so that every entry is in range
-  for (long long n = nFluid; n < nCells; ++n)
-    for (int q = 0; q < QM; ++q) adj[(size_t)n * QM + q] = (uint32_t)(lbm::inv(q) * nCells + n);
-
   BCK(cudaMalloc(&d.pdfs, (size_t)nCells * Q * b->elemBytes));
   BCK(cudaMalloc(&d.adj, (size_t)nCells * QM * 4));
-  BCK(cudaMemcpyAsync(d.adj, adj.data(), adj.size() * 4, cudaMemcpyHostToDevice, b->stream));
+  // numbering and adjacency built on the device (lbm_build.cu); padding
+  // nodes then point at their own slots so that every entry is in range
+  int* dMask = nullptr;
+  uint32_t* dGrid = nullptr;
+  BCK(cudaMallocAsync(&dMask, sizeof(int) * ncell, b->stream));
+  BCK(cudaMallocAsync(&dGrid, sizeof(uint32_t) * ncell, b->stream));
+  BCK(cudaMemcpyAsync(dMask, ld->Lattice, sizeof(int) * ncell, cudaMemcpyHostToDevice, b->stream));
+  const int blk[3] = {0, 0, 0}, per[3] = {ld->PeriodicX, ld->PeriodicY, ld->PeriodicZ};
+  const char* berr = "";
+  const long long nf = lbm::list_build_device(dMask, ld->Dims, per, 0, blk, (int)nCells, dGrid, d.adj, nCells,
+                                              b->stream, &berr);
+  if (nf == nFluid) {
+    lbm::batch_pad_adjacency(d.adj, nFluid, nCells, b->stream);
+    BCK(cudaMemcpyAsync(d.grid.data(), dGrid, sizeof(uint32_t) * ncell, cudaMemcpyDeviceToHost, b->stream));
+  }
+  cudaFreeAsync(dGrid, b->stream);
+  cudaFreeAsync(dMask, b->stream);
+  BCK(cudaStreamSynchronize(b->stream));
+  if (nf != nFluid) {
+    g_batchError = nf < 0 ? berr : "the mask's fluid cell count differs from the lattice's";
+    cudaFree(d.pdfs);
+    cudaFree(d.adj);
+    d = DomainSlot();
+    return -6;
+  }
   d.active = true;
   d.bytes = bytes;
   d.nTiles = (int)(nCells / lbm::kBatchTileNodes);

@@ -60,6 +60,11 @@ struct BatchLaunch {
   int blocks;          // persistent grid size; 0 = one block per tile
 };
 
+// Adjacency rows of the padding nodes [nFluid, nCells): each entry points at
+// the node's own slot of the inverse direction (always in range, never read
+// back into a fluid node).
+void batch_pad_adjacency(uint32_t* adj, int nFluid, long long nCells, cudaStream_t s);
+
 // Builds the tile records of tiles [0, nTiles).
 void batch_build_tiles(const BatchDomain* doms, const int* tileDom, int nTiles, BatchTile* out, cudaStream_t s);
 

@@ -239,6 +239,18 @@ __global__ void k_batch_tiles(const BatchDomain* doms, const int* tileDom, int n
   out[t] = r;
 }
 
+__global__ void k_batch_pad_adjacency(uint32_t* adj, int nFluid, long long nCells) {
+  const long long n = nFluid + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= nCells) return;
+#pragma unroll
+  for (int q = 0; q < QM; ++q) adj[n * QM + q] = (uint32_t)(inv(q) * nCells + n);
+}
+
+void batch_pad_adjacency(uint32_t* adj, int nFluid, long long nCells, cudaStream_t s) {
+  const long long pad = nCells - nFluid;
+  if (pad > 0) k_batch_pad_adjacency<<<(unsigned)((pad + 255) / 256), 256, 0, s>>>(adj, nFluid, nCells);
+}
+
 void batch_build_tiles(const BatchDomain* doms, const int* tileDom, int nTiles, BatchTile* out, cudaStream_t s) {
   if (nTiles > 0) k_batch_tiles<<<(nTiles + 255) / 256, 256, 0, s>>>(doms, tileDom, nTiles, out);
 }

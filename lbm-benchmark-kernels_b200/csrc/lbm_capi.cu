@@ -10,6 +10,7 @@
 // The host keeps a pinned mirror of the current PDF array for
 // GetNode/SetNode; Kernel uploads it when SetNode has touched it, runs the time
 // steps back to back on the instance's stream, and downloads it afterwards.
+#include <algorithm>
 #include <cerrno>
 #include <chrono>
 #include <cstdio>
@@ -256,7 +257,12 @@ lbm::AaArgs aa_args(Gpu* g) {
   a.perX = g->per[0];
   a.perY = g->per[1];
   a.perZ = g->per[2];
-  for (int d = 0; d < Q; ++d) a.plane[d] = g->dF + d * g->dstride;
+  const int S = (int)g->dstride;
+  for (int d = 0; d < Q; ++d) {
+    const int j = lbm::inv(d);
+    a.ldOff[d] = d == lbm::DC ? lbm::DC * S : j * S + lbm::cx(j) * g->xs + lbm::cy(j) * g->pitch + lbm::cz(j);
+    a.stOff[d] = d == lbm::DC ? lbm::DC * S : d * S + lbm::cx(d) * g->xs + lbm::cy(d) * g->pitch + lbm::cz(d);
+  }
   return a;
 }
 
@@ -524,6 +530,12 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params) {
     g->pitch = (ld->Dims[2] + lbm::kZOff + 1 + 3) / 4 * 4;
     g->xs = gy * g->pitch;
     g->dstride = (long long)gx * g->xs;
+    if ((unsigned long long)Q * g->dstride >= (1ull << 31)) {
+      // the odd step addresses all 19 planes with 32-bit offsets (the
+      // reference bounds its PDF count by 2^31 too, src/Main.c:399-406)
+      std::printf("ERROR: the full-array layout of this lattice exceeds 2^31 PDFs; use a list kernel.\n");
+      std::exit(1);
+    }
     g->mirrorElems = (size_t)Q * g->dstride;
     kd->GlobalDims[0] = gx;
     kd->GlobalDims[1] = gy;
@@ -558,18 +570,36 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params) {
     int nCells = lbmh_pad_cells(ld->nFluid, (int)sizeof(double), a.pad);
     if (nCells < 0) std::exit(1);
     if (pull) nCells = nCells + (8 - nCells % 8);  // cache-line pad (src/BenchKernelD3Q19ListPullSplitNtCommon.c:494-496)
+    if (a.storage != lbm::kStoreF64)
+      // reduced storage: planes padded to whole staging tiles (-pad does not apply)
+      nCells = (std::max(ld->nFluid, 1) + lbm::kLpTileNodes - 1) / lbm::kLpTileNodes * lbm::kLpTileNodes;
     g->nCells = nCells;
     g->nFluid = ld->nFluid;
     const long ncell = (long)ld->Dims[0] * ld->Dims[1] * ld->Dims[2];
     g->grid = static_cast<uint32_t*>(std::malloc(sizeof(uint32_t) * ncell));
+    if (!g->grid) { std::printf("ERROR: allocation failed.\n"); std::exit(1); }
     const long nTiles = (g->nFluid + lbm::kListTile - 1) / lbm::kListTile;
     const size_t adjElems = (size_t)(nTiles > 0 ? nTiles : 1) * lbm::kListTile * QM;
-    g->adjHost = static_cast<uint32_t*>(std::calloc(adjElems, sizeof(uint32_t)));
-    if (!g->grid || !g->adjHost) { std::printf("ERROR: allocation failed.\n"); std::exit(1); }
-    const int nf = lbmh_list_build(ld, pull ? 1 : 0, a.blk, nCells, g->grid, nullptr, g->adjHost);
-    if (nf != g->nFluid) { std::printf("ERROR: fluid node count mismatch.\n"); std::exit(1); }
+    // numbering and adjacency built on the device (lbm_build.cu); the host
+    // keeps the numbering for GetNode/SetNode
     LBM_CK(cudaMalloc(&g->dAdj, sizeof(uint32_t) * adjElems));
-    LBM_CK(cudaMemcpy(g->dAdj, g->adjHost, sizeof(uint32_t) * adjElems, cudaMemcpyHostToDevice));
+    LBM_CK(cudaMemset(g->dAdj, 0, sizeof(uint32_t) * adjElems));
+    int* dMask = nullptr;
+    uint32_t* dGrid = nullptr;
+    LBM_CK(cudaMalloc(&dMask, sizeof(int) * ncell));
+    LBM_CK(cudaMalloc(&dGrid, sizeof(uint32_t) * ncell));
+    LBM_CK(cudaMemcpy(dMask, ld->Lattice, sizeof(int) * ncell, cudaMemcpyHostToDevice));
+    const int per3[3] = {ld->PeriodicX, ld->PeriodicY, ld->PeriodicZ};
+    const char* berr = "";
+    const long long nf = lbm::list_build_device(dMask, ld->Dims, per3, pull ? 1 : 0, a.blk, nCells, dGrid, g->dAdj,
+                                                nTiles * lbm::kListTile, g->stream, &berr);
+    if (nf != g->nFluid) {
+      std::printf("ERROR: list build: %s (fluid nodes %lld, expected %d).\n", berr, nf, g->nFluid);
+      std::exit(1);
+    }
+    LBM_CK(cudaMemcpy(g->grid, dGrid, sizeof(uint32_t) * ncell, cudaMemcpyDeviceToHost));
+    LBM_CK(cudaFree(dGrid));
+    LBM_CK(cudaFree(dMask));
     g->mirrorElems = (size_t)Q * nCells;
     LBM_CK(cudaMalloc(&g->dF, g->elemBytes * g->mirrorElems));
     LBM_CK(cudaMemset(g->dF, 0, g->elemBytes * g->mirrorElems));
@@ -901,6 +931,17 @@ void lbm_b200_set_field(KernelData* kd, LatticeDesc* ld, const double* in) {
 int lbm_b200_list_layout(KernelData* kd, const uint32_t** grid, const uint32_t** adj, int* nFluid, int* nCells) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
   if (g->kind == kAa) return -1;
+  if (adj && !g->adjHost && g->nFluid > 0) {
+    // the adjacency lives on the device; a host copy is made on first request
+    g->adjHost = static_cast<uint32_t*>(std::malloc(sizeof(uint32_t) * (size_t)g->nFluid * QM));
+    if (!g->adjHost ||
+        cudaMemcpy(g->adjHost, g->dAdj, sizeof(uint32_t) * (size_t)g->nFluid * QM, cudaMemcpyDeviceToHost) !=
+            cudaSuccess) {
+      std::free(g->adjHost);
+      g->adjHost = nullptr;
+      return -2;
+    }
+  }
   if (grid) *grid = g->grid;
   if (adj) *adj = g->adjHost;
   if (nFluid) *nFluid = g->nFluid;

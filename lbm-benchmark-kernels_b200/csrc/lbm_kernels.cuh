@@ -35,7 +35,10 @@ struct AaArgs {
   int nX, nY, nZ;
   int xs, pitch;
   int perX, perY, perZ;
-  double* plane[Q];  // f + d * dstride: one address add per access from the parameter bank
+  // element offsets from a cell's slot of plane 0, per direction d, read from
+  // the parameter bank: the odd step's load of d (slot inv(d) of x + c_inv(d))
+  // and store of d (slot d of x + c_d); the centre uses its own slot
+  int ldOff[Q], stOff[Q];
 };
 
 // ---------------------------------------------------------------------------
@@ -63,6 +66,11 @@ constexpr int kStoreF64 = 0;
 constexpr int kStoreF32 = 1;
 constexpr int kStoreF16 = 2;
 
+// Plane stride granularity of the reduced-storage list layout: nCells is a
+// multiple of this, so that every plane segment of an even-step tile is one
+// aligned bulk copy inside the array.
+constexpr int kLpTileNodes = 1024;
+
 struct ListArgsLp {
   void* f;  // float or __half, f[d * nCells + n]
   const uint32_t* adj;
@@ -70,6 +78,13 @@ struct ListArgsLp {
   int nFluid;
   int* err;
 };
+
+// List layout built on the device (lbm_build.cu): numbering into grid (one
+// entry per cell), adjacency for up to adjCap nodes. Synchronises s. Returns
+// the fluid node count, -1 on a CUDA error, -2 if adjCap is too small.
+long long list_build_device(const int* mask, const int dims[3], const int periodic[3], int pull, const int blk[3],
+                            int nCells, uint32_t* grid, uint32_t* adj, long long adjCap, cudaStream_t s,
+                            const char** err);
 
 // Launchers (stream-ordered, no synchronisation).
 void list_even_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s);

@@ -108,8 +108,14 @@ __device__ __forceinline__ void aa_interior_block(const AaArgs& a, int id, int& 
   x = 1 + rest / gy;
 }
 
+// Launch bounds: the direct kernel is capped at 7 resident blocks of 128
+// threads per SM (68 registers, no spills), the general one at 5 (96); both
+// measured fastest among 1-8 on B200. Addresses are the cell's base pointer
+// plus a per-direction offset from the parameter bank (and the z wrap), so no
+// per-direction address stays live in registers.
 template <bool kDirect>
-__global__ void __launch_bounds__(128) k_aa_odd_interior_fp64(const AaArgs a, const Trt<double> t, const int* blocks) {
+__global__ void __launch_bounds__(128, kDirect ? 7 : 5)
+    k_aa_odd_interior_fp64(const AaArgs a, const Trt<double> t, const int* blocks) {
   int x, y, z;
   aa_interior_block(a, blocks[blockIdx.x], z, y, x);
   const int zHi = a.perZ ? a.nZ - 1 : a.nZ - 2;
@@ -117,34 +123,34 @@ __global__ void __launch_bounds__(128) k_aa_odd_interior_fp64(const AaArgs a, co
   const int c = aa_cell(a, x, y, z);
   const uint32_t w = __ldg(a.link + c);
   if (!(w & kFluidBit)) return;
+  double* const fb = a.f + c;
   // the periodic z wrap, decided once per cell: a link with c_z = -1 leaving
   // through z = 0 moves +nZ cells, one with c_z = +1 through z = nZ-1 moves -nZ
   const int wrapDown = z == 0 ? a.nZ : 0, wrapUp = z == a.nZ - 1 ? -a.nZ : 0;
-  auto nbr = [&](int d) -> int {
-    return c + aa_off(a, d) + (cz(d) < 0 ? wrapDown : (cz(d) > 0 ? wrapUp : 0));
-  };
+  auto wrap = [&](int d) -> int { return cz(d) < 0 ? wrapDown : (cz(d) > 0 ? wrapUp : 0); };
   if (kDirect) {
-    // store addresses come from laundered plane pointers, apart from the load
+    // store addresses come from a laundered base pointer, apart from the load
     // addresses, so those need not stay live across the collision
-    trt_update(
-        t, [&](int d) -> double { return a.plane[inv(d)][d == DC ? c : nbr(inv(d))] + t.force[d]; },
-        [&](int d, double v) { launder(a.plane[d])[d == DC ? c : nbr(d)] = v + t.force[d]; });
+    trt_update(t, [&](int d) -> double { return fb[a.ldOff[d] + wrap(inv(d))] + t.force[d]; },
+               [&](int d, double v) { launder(fb)[a.stOff[d] + wrap(d)] = v + t.force[d]; });
     return;
   }
+  const int S = (int)a.dstride;
   auto load = [&](int d) -> double {
-    if (d == DC) return a.plane[DC][c] + t.force[DC];
+    if (d == DC) return fb[a.ldOff[DC]] + t.force[DC];
     const int j = inv(d);
     const bool rev = (w >> j) & 1u;
-    return (rev ? a.plane[d] + c : a.plane[j] + nbr(j))[0] + t.force[d];
+    return fb[rev ? d * S : a.ldOff[d] + wrap(j)] + t.force[d];
   };
   auto store = [&](int d, double v) {
+    double* const fs = launder(fb);
     if (d == DC) {
-      launder(a.plane[DC])[c] = v + t.force[DC];
+      fs[a.stOff[DC]] = v + t.force[DC];
       return;
     }
     const int j = inv(d);
     const bool rev = (w >> d) & 1u;
-    (rev ? launder(a.plane[j]) + c : launder(a.plane[d]) + nbr(d))[0] = v + (rev ? t.force[j] : t.force[d]);
+    fs[rev ? j * S : a.stOff[d] + wrap(d)] = v + (rev ? t.force[j] : t.force[d]);
   };
   trt_update(t, load, store);
 }

@@ -20,6 +20,67 @@ __global__ void __launch_bounds__(kListTile) k_list_even_lp(const ListArgsLp a, 
              [&](int d, float v) { fs[inv(d) * S] = St::raw(v, inv(d)); });
 }
 
+// Even step with the PDF planes staged through shared memory by bulk copies
+// (TMA, cp.async.bulk): each tile of TN = StageBytes / sizeof(T) nodes is 19
+// contiguous plane segments, copied by one thread into one of Stages buffers
+// with an mbarrier per buffer; Stages - 1 tiles are in flight while one is
+// relaxed, so the bytes in flight per SM do not depend on registers. Stores
+// go straight to global memory (coalesced, swapped planes). Requires the
+// plane stride nCells to be a multiple of TN (the reduced-storage layout pads
+// it to whole kLpTileNodes tiles).
+template <class St, int StageBytes, int Stages>
+__global__ void __launch_bounds__(256) k_list_even_staged(const ListArgsLp a, const Trt<float> t) {
+  using T = typename St::T;
+  constexpr int TN = StageBytes / (int)sizeof(T);
+  constexpr int NPT = TN / 256;
+  static_assert(TN % 256 == 0 && StageBytes % 16 == 0, "stage layout");
+  extern __shared__ __align__(128) unsigned char stage[];  // Stages x Q x StageBytes
+  __shared__ alignas(8) uint64_t full[Stages];
+  const int nTiles = (a.nFluid + TN - 1) / TN;
+  T* const f = static_cast<T*>(a.f);
+  const long long S = a.nCells;
+  auto issue = [&](int tile, int st) {  // thread 0
+    mbar_arrive_expect_tx(&full[st], Q * StageBytes);
+    unsigned char* dst = stage + (size_t)st * Q * StageBytes;
+    for (int d = 0; d < Q; ++d) bulk_g2s(dst + d * StageBytes, f + d * S + (long long)tile * TN, StageBytes, &full[st]);
+  };
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < Stages; ++st) mbar_init(&full[st], 1);
+    for (int st = 0; st < Stages - 1; ++st)
+      if (blockIdx.x + st * gridDim.x < nTiles) issue(blockIdx.x + st * gridDim.x, st);
+  }
+  int i = 0;
+  for (int tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++i) {
+    const int st = i % Stages;
+    __syncthreads();  // the buffer refilled below was read by everyone in the previous iteration
+    if (threadIdx.x == 0) {
+      const long long ahead = tile + (long long)(Stages - 1) * gridDim.x;
+      if (ahead < nTiles) issue((int)ahead, (i + Stages - 1) % Stages);
+    }
+    if (!mbar_wait_bounded(&full[st], (i / Stages) & 1)) {
+      if (threadIdx.x == 0) {
+        atomicOr(a.err, 1);
+        // let the copies already issued for later tiles land before the
+        // block's shared memory is released
+        for (int j = 1; j < Stages; ++j)
+          if (tile + (long long)j * gridDim.x < nTiles)
+            mbar_wait_bounded(&full[(i + j) % Stages], ((i + j) / Stages) & 1);
+      }
+      return;
+    }
+    const T* buf = reinterpret_cast<const T*>(stage + (size_t)st * Q * StageBytes);
+#pragma unroll 1
+    for (int k = 0; k < NPT; ++k) {
+      const int local = threadIdx.x + k * 256;
+      const int n = tile * TN + local;
+      if (n >= a.nFluid) break;
+      T* const fs = launder(f + n);
+      trt_update(t, [&](int d) { return St::dev(buf[d * TN + local], d); },
+                 [&](int d, float v) { fs[inv(d) * S] = St::raw(v, inv(d)); });
+    }
+  }
+}
+
 __device__ __forceinline__ bool stage_adj_tile_lp(const ListArgsLp& a, uint32_t* sadj, uint64_t* bar) {
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
@@ -61,12 +122,36 @@ __global__ void __launch_bounds__(kListTile) k_list_odd_lp(const ListArgsLp a, c
 
 static unsigned lp_blocks(const ListArgsLp& a) { return (a.nFluid + kListTile - 1) / kListTile; }
 
+// Staging geometry of the even step: 2 KB plane segments (1024 FP16 or 512
+// FP32 nodes per tile), 2 buffers, 2 resident blocks of 256 threads per SM.
+constexpr int kEvenStageBytes = 2048, kEvenStages = 2, kEvenBlocksPerSM = 2;
+
+// The kernel's shared-memory opt-in is a per-device attribute: it is set once
+// per device (and per storage type), with the grid sized to that device.
+template <class St>
+static void launch_even_staged(const ListArgsLp& a, const Trt<float>& t, cudaStream_t s) {
+  constexpr int kMaxDevices = 64;
+  static int grid[kMaxDevices] = {0};
+  constexpr size_t smem = (size_t)kEvenStages * Q * kEvenStageBytes;
+  auto kern = k_list_even_staged<St, kEvenStageBytes, kEvenStages>;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int& g = grid[dev < kMaxDevices ? dev : 0];
+  if (g == 0 || dev >= kMaxDevices) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    g = sms * kEvenBlocksPerSM;
+  }
+  kern<<<g, 256, smem, s>>>(a, t);
+}
+
 void list_even_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s) {
   if (a.nFluid <= 0) return;
   if (storage == kStoreF16)
-    k_list_even_lp<StoreF16><<<lp_blocks(a), kListTile, 0, s>>>(a, t);
+    launch_even_staged<StoreF16>(a, t, s);
   else
-    k_list_even_lp<StoreF32><<<lp_blocks(a), kListTile, 0, s>>>(a, t);
+    launch_even_staged<StoreF32>(a, t, s);
 }
 
 void list_odd_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s) {

@@ -344,6 +344,25 @@ def list_build(lattice, pull, blk=(0, 0, 0), pad=None):
     return grid, adj[: nf * 18], nf, n_cells
 
 
+def list_build_device(lattice, pull, blk=(0, 0, 0), pad=None):
+    """lbm_b200_list_build: the same layout built on the GPU."""
+    L = lib()
+    n_cells = L.lbmh_pad_cells(lattice.n_fluid, 8, pad.encode() if pad else None)
+    if n_cells < 0:
+        raise ValueError("bad padding string %r" % pad)
+    if pull:
+        n_cells = n_cells + (8 - n_cells % 8)
+    grid = np.zeros(lattice.mask.size, dtype=np.uint32)
+    adj = np.zeros(max(lattice.n_fluid, 1) * 18, dtype=np.uint32)
+    b = (ctypes.c_int * 3)(*blk)
+    nf = L.lbm_b200_list_build(ctypes.byref(lattice.desc), int(bool(pull)), b, n_cells,
+                               grid.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                               adj.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+    if nf < 0:
+        raise RuntimeError("device list build failed (%d)" % nf)
+    return grid, adj[: nf * 18], nf, n_cells
+
+
 # ---------------------------------------------------------------------------
 # Batched domains (lbm_batch_* in include/lbm_b200.h)
 
