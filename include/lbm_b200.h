@@ -131,6 +131,24 @@ void D3Q19CudaListPullSplitNt1SInit_PullSoA(LatticeDesc *ld, KernelData **kernel
 void D3Q19CudaListPullSplitNt2SInit_PullSoA(LatticeDesc *ld, KernelData **kernelData, Parameters *params);
 void D3Q19CudaListPullSplitNtDeinit_PullSoA(LatticeDesc *ld, KernelData **kernelData);
 
+/* "cuda-list-aa-soa" / "cuda-list-aa-ria-soa": the reference's other list-AA
+ * rows (src/KernelFunctions.h:63-72: D3Q19ListAaInit_PushSoA,
+ * D3Q19ListAaRiaInit_PushSoA and their Deinit). Same layout and arithmetic as
+ * list-aa-pv-soa; on the GPU they run the list AA kernels. */
+void D3Q19CudaListAaInit_PushSoA(LatticeDesc *ld, KernelData **kernelData, Parameters *params);
+void D3Q19CudaListAaDeinit_PushSoA(LatticeDesc *ld, KernelData **kernelData);
+void D3Q19CudaListAaRiaInit_PushSoA(LatticeDesc *ld, KernelData **kernelData, Parameters *params);
+void D3Q19CudaListAaRiaDeinit_PushSoA(LatticeDesc *ld, KernelData **kernelData);
+
+/* "cuda-list-push-soa" / "cuda-list-pull-soa": two-grid list kernels, push or
+ * pull adjacency, SoA padding without the pull-split cache-line pad. Replace
+ * D3Q19ListInit_PushSoA / D3Q19ListInit_PullSoA and their Deinit
+ * (src/BenchKernelD3Q19List.c, registered at src/KernelFunctions.h:106-120). */
+void D3Q19CudaListInit_PushSoA(LatticeDesc *ld, KernelData **kernelData, Parameters *params);
+void D3Q19CudaListDeinit_PushSoA(LatticeDesc *ld, KernelData **kernelData);
+void D3Q19CudaListInit_PullSoA(LatticeDesc *ld, KernelData **kernelData, Parameters *params);
+void D3Q19CudaListDeinit_PullSoA(LatticeDesc *ld, KernelData **kernelData);
+
 /* The rows above as a table: {Name, Init, Deinit}, in the layout of the
  * reference's KernelFunctions (src/KernelFunctions.h:49-54). */
 typedef struct LbmB200KernelFunctions_ {

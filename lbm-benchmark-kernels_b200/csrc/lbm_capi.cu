@@ -28,7 +28,11 @@ namespace {
 using lbm::Q;
 using lbm::QM;
 
-enum Kind { kAa = 0, kListAa = 1, kListPull = 2 };
+// kListPull: pull-split layout (with its cache-line pad); kListPullPlain and
+// kListPush: the two-grid list kernels list-pull-soa / list-push-soa
+enum Kind { kAa = 0, kListAa = 1, kListPull = 2, kListPullPlain = 3, kListPush = 4 };
+
+bool two_grid(int kind) { return kind == kListPull || kind == kListPullPlain || kind == kListPush; }
 
 thread_local std::string g_lastError;
 
@@ -287,7 +291,7 @@ lbm::ListArgsLp list_args_lp(Gpu* g) {
   return a;
 }
 
-double* current_grid(Gpu* g) { return (g->kind == kListPull && g->cur == 1) ? g->dG : g->dF; }
+double* current_grid(Gpu* g) { return (two_grid(g->kind) && g->cur == 1) ? g->dG : g->dF; }
 
 // Enqueues n time steps (AA kernels: rounded up to whole even/odd pairs, as
 // the reference's loop `for (iter = 0; iter < n; iter += 2)`); returns the
@@ -349,7 +353,10 @@ long enqueue_steps(Gpu* g, const lbm::Trt<double>& t, int n, cudaEvent_t* ev = n
     for (int it = 0; it < n; ++it) {
       lbm::ListArgs a = list_args(g);
       mark();
-      lbm::list_pull_fp64(a, t, g->stream);
+      if (g->kind == kListPush)
+        lbm::list_push_fp64(a, t, g->stream);
+      else
+        lbm::list_pull_fp64(a, t, g->stream);
       ++k;
       g->cur ^= 1;
       g->iteration = it;
@@ -360,7 +367,7 @@ long enqueue_steps(Gpu* g, const lbm::Trt<double>& t, int n, cudaEvent_t* ev = n
 }
 
 long launches_for(Gpu* g, int n) {
-  if (g->kind == kListPull) return n;
+  if (two_grid(g->kind)) return n;
   long perPair = 2;
   if (g->kind == kAa) {
     const lbm::AaArgs a = aa_args(g);
@@ -443,7 +450,7 @@ void vtk_or_exit(LatticeDesc* ld, KernelData* kd, CaseData* cd, int label) {
 // synchronises and downloads the mirror; the final dump follows the timed
 // region.
 long enqueue_steps_vtk(LatticeDesc* ld, Gpu* g, CaseData* cd, const lbm::Trt<double>& t) {
-  const int n = cd->MaxIterations, stride = g->kind == kListPull ? 1 : 2;
+  const int n = cd->MaxIterations, stride = two_grid(g->kind) ? 1 : 2;
   const int modulus = cd->VtkModulus > 0 ? cd->VtkModulus : 1;
   long k = 0;
   for (int it = 0; it < n; it += stride) {
@@ -566,10 +573,10 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params) {
     }
     std::free(link);
   } else {
-    const bool pull = kind == kListPull;
+    const bool pull = kind == kListPull || kind == kListPullPlain;
     int nCells = lbmh_pad_cells(ld->nFluid, (int)sizeof(double), a.pad);
     if (nCells < 0) std::exit(1);
-    if (pull) nCells = nCells + (8 - nCells % 8);  // cache-line pad (src/BenchKernelD3Q19ListPullSplitNtCommon.c:494-496)
+    if (kind == kListPull) nCells = nCells + (8 - nCells % 8);  // cache-line pad (src/BenchKernelD3Q19ListPullSplitNtCommon.c:494-496)
     if (a.storage != lbm::kStoreF64)
       // reduced storage: planes padded to whole staging tiles (-pad does not apply)
       nCells = (std::max(ld->nFluid, 1) + lbm::kLpTileNodes - 1) / lbm::kLpTileNodes * lbm::kLpTileNodes;
@@ -603,7 +610,7 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params) {
     g->mirrorElems = (size_t)Q * nCells;
     LBM_CK(cudaMalloc(&g->dF, g->elemBytes * g->mirrorElems));
     LBM_CK(cudaMemset(g->dF, 0, g->elemBytes * g->mirrorElems));
-    if (pull) {
+    if (two_grid(kind)) {
       LBM_CK(cudaMalloc(&g->dG, sizeof(double) * g->mirrorElems));
       LBM_CK(cudaMemset(g->dG, 0, sizeof(double) * g->mirrorElems));
     }
@@ -612,7 +619,7 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params) {
     kd->GlobalDims[2] = ld->Dims[2];
     // the GPU odd step reads all 18 adjacency entries of a node every time
     const double pb = 2.0 * 19 * (double)g->elemBytes;
-    kd->LoopBalance = pull ? pb + 18 * 4.0 : (pb + (pb + 18 * 4.0)) / 2.0;
+    kd->LoopBalance = two_grid(kind) ? pb + 18 * 4.0 : (pb + (pb + 18 * 4.0)) / 2.0;
   }
 
   LBM_CK(cudaMallocHost(&g->mirror, sizeof(double) * g->mirrorElems));
@@ -731,11 +738,44 @@ void D3Q19CudaListPullSplitNtDeinit_PullSoA(LatticeDesc* ld, KernelData** kernel
   gpu_free(kernelData);
 }
 
+void D3Q19CudaListAaInit_PushSoA(LatticeDesc* ld, KernelData** kernelData, Parameters* params) {
+  *kernelData = &gpu_new(kListAa, ld, params)->kd;
+}
+void D3Q19CudaListAaDeinit_PushSoA(LatticeDesc* ld, KernelData** kernelData) {
+  (void)ld;
+  gpu_free(kernelData);
+}
+void D3Q19CudaListAaRiaInit_PushSoA(LatticeDesc* ld, KernelData** kernelData, Parameters* params) {
+  *kernelData = &gpu_new(kListAa, ld, params)->kd;
+}
+void D3Q19CudaListAaRiaDeinit_PushSoA(LatticeDesc* ld, KernelData** kernelData) {
+  (void)ld;
+  gpu_free(kernelData);
+}
+void D3Q19CudaListInit_PushSoA(LatticeDesc* ld, KernelData** kernelData, Parameters* params) {
+  *kernelData = &gpu_new(kListPush, ld, params)->kd;
+}
+void D3Q19CudaListDeinit_PushSoA(LatticeDesc* ld, KernelData** kernelData) {
+  (void)ld;
+  gpu_free(kernelData);
+}
+void D3Q19CudaListInit_PullSoA(LatticeDesc* ld, KernelData** kernelData, Parameters* params) {
+  *kernelData = &gpu_new(kListPullPlain, ld, params)->kd;
+}
+void D3Q19CudaListDeinit_PullSoA(LatticeDesc* ld, KernelData** kernelData) {
+  (void)ld;
+  gpu_free(kernelData);
+}
+
 static const LbmB200KernelFunctions kTable[] = {
     {"cuda-aa-soa", D3Q19CudaAaInit_AaSoA, D3Q19CudaAaDeinit_AaSoA},
     {"cuda-list-aa-pv-soa", D3Q19CudaListAaPvInit_PushSoA, D3Q19CudaListAaPvDeinit_PushSoA},
     {"cuda-list-pull-split-nt-1s-soa", D3Q19CudaListPullSplitNt1SInit_PullSoA, D3Q19CudaListPullSplitNtDeinit_PullSoA},
     {"cuda-list-pull-split-nt-2s-soa", D3Q19CudaListPullSplitNt2SInit_PullSoA, D3Q19CudaListPullSplitNtDeinit_PullSoA},
+    {"cuda-list-aa-soa", D3Q19CudaListAaInit_PushSoA, D3Q19CudaListAaDeinit_PushSoA},
+    {"cuda-list-aa-ria-soa", D3Q19CudaListAaRiaInit_PushSoA, D3Q19CudaListAaRiaDeinit_PushSoA},
+    {"cuda-list-push-soa", D3Q19CudaListInit_PushSoA, D3Q19CudaListDeinit_PushSoA},
+    {"cuda-list-pull-soa", D3Q19CudaListInit_PullSoA, D3Q19CudaListDeinit_PullSoA},
 };
 
 const LbmB200KernelFunctions* lbm_b200_kernels(int* count) {

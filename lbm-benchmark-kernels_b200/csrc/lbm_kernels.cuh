@@ -107,6 +107,7 @@ long long aa_shell_cells(const AaArgs& a);
 void list_even_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
 void list_odd_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
 void list_pull_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
+void list_push_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
 
 // FP64 mass and momentum sums of a list-layout field (lbm_moments.cu):
 // pass 1 writes 4 partial sums per block of kListTile nodes into `partials`

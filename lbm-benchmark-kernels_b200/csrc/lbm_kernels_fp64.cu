@@ -362,6 +362,31 @@ __global__ void __launch_bounds__(kListTile) k_list_pull_fp64(const ListArgs a, 
   for (int d = 0; d < Q; ++d) a.g[d * S + n] = o[d] + t.force[d];
 }
 
+// Two-grid list push (src/BenchKernelD3Q19List.c:114-320, PROP_MODEL_PUSH):
+// the node's own 19 PDFs from the source grid, each post-collision PDF
+// written through the push adjacency into the destination grid with the
+// body-force increment of the slot's direction (a bounce back lands in the
+// node's own slot inv(d) and gets the increment of inv(d)).
+__global__ void __launch_bounds__(kListTile, 3) k_list_push_fp64(const ListArgs a, const Trt<double> t) {
+  __shared__ alignas(128) uint32_t sadj[kListTile * QM];
+  __shared__ alignas(8) uint64_t bar;
+  if (!stage_adj_tile(a, sadj, &bar)) return;
+  const int n = blockIdx.x * kListTile + threadIdx.x;
+  if (n >= a.nFluid) return;
+  const uint32_t* e = sadj + threadIdx.x * QM;
+  const double* const f = a.f + n;
+  double* const g = a.g;
+  const long long S = a.nCells;
+  auto store = [&](int d, double v) {
+    if (d == DC) { g[DC * S + n] = v + t.force[DC]; return; }
+    const uint32_t dst = reinterpret_cast<const volatile uint32_t*>(e)[d];
+    const int j = inv(d);
+    const bool bounce = dst == static_cast<uint32_t>(j * S + n);
+    g[dst] = v + (bounce ? t.force[j] : t.force[d]);
+  };
+  trt_update(t, [&](int d) { return f[d * S]; }, store);
+}
+
 static unsigned list_blocks(const ListArgs& a) { return (a.nFluid + kListTile - 1) / kListTile; }
 
 void list_even_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s) {
@@ -372,6 +397,9 @@ void list_odd_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s) {
 }
 void list_pull_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s) {
   if (a.nFluid > 0) k_list_pull_fp64<<<list_blocks(a), kListTile, 0, s>>>(a, t);
+}
+void list_push_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s) {
+  if (a.nFluid > 0) k_list_push_fp64<<<list_blocks(a), kListTile, 0, s>>>(a, t);
 }
 
 }  // namespace lbm

@@ -146,12 +146,15 @@ static void launch_even_staged(const ListArgsLp& a, const Trt<float>& t, cudaStr
   kern<<<g, 256, smem, s>>>(a, t);
 }
 
+// FP16: the staged even step (0.118 -> 0.100 ms at 6.7M nodes on B200, 66 ->
+// 78 % of the measured HBM bandwidth). FP32: the direct kernel, whose 4-byte
+// loads already keep enough bytes in flight (0.162 ms direct, 0.174 staged).
 void list_even_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s) {
   if (a.nFluid <= 0) return;
   if (storage == kStoreF16)
     launch_even_staged<StoreF16>(a, t, s);
   else
-    launch_even_staged<StoreF32>(a, t, s);
+    k_list_even_lp<StoreF32><<<lp_blocks(a), kListTile, 0, s>>>(a, t);
 }
 
 void list_odd_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s) {

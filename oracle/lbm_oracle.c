@@ -12,6 +12,8 @@
  *                       path arithmetic)
  *   list pull-split     src/BenchKernelD3Q19ListPullSplitNtCommon.c:422-797,
  *                       src/BenchKernelD3Q19ListPullSplitNt1SScalar.h
+ *   list push/pull      src/BenchKernelD3Q19ListCommon.c:330-600 (layout),
+ *   (two grids)         src/BenchKernelD3Q19List.c:114-344 (steps)
  *   body force          src/Kernel.c:759-803
  *   -verify init/check  src/Kernel.c:258-438, 451-625
  * The TRT magic parameter is an argument here (the reference hard-codes 1/12,
@@ -198,6 +200,8 @@ typedef struct {
 	uint32_t *grid, *coords, *adj;
 } orc_list_t;
 
+/* pull: 1 pull adjacency with the pull-split cache-line pad, 2 pull adjacency
+ * without it (two-grid list-pull-soa), 0 push adjacency. */
 static int list_build(orc_list_t *L, int pull, const int dims[3], const int periodic[3], const int *lat,
                       const int blk_in[3], int pad_mode, int n_pairs, const int *modulus, const int *offset)
 {
@@ -208,7 +212,7 @@ static int list_build(orc_list_t *L, int pull, const int dims[3], const int peri
 
 	int nCells = orc_pad_cells(nf, 8, pad_mode, n_pairs, modulus, offset);
 	if (nCells < 0) return -1;
-	if (pull) nCells = nCells + (8 - nCells % 8);
+	if (pull == 1) nCells = nCells + (8 - nCells % 8);
 
 	L->nx = nx; L->ny = ny; L->nz = nz; L->nFluid = nf; L->nCells = nCells;
 	L->grid = (uint32_t *)malloc(n * sizeof(uint32_t));
@@ -518,6 +522,23 @@ static void list_pull(orc_state_t *s, const trt_t *t)
 	}
 }
 
+/* Two-grid list push (src/BenchKernelD3Q19List.c:114-320, PROP_MODEL_PUSH):
+ * the node's own PDFs from the source grid, each post-collision PDF written
+ * through the push adjacency into the destination grid. */
+static void list_push2(orc_state_t *s, const trt_t *t)
+{
+	size_t nc = (size_t)s->L.nCells;
+	#pragma omp parallel for
+	for (int n = 0; n < s->L.nFluid; ++n) {
+		const uint32_t *a = s->L.adj + (size_t)n * QM;
+		double f[Q], o[Q];
+		for (int d = 0; d < Q; ++d) f[d] = s->f[d * nc + n];
+		trt_collide(t, f, o);
+		for (int d = 0; d < QM; ++d) s->g[a[d]] = o[d];
+		s->g[DC * nc + n] = o[DC];
+	}
+}
+
 /* ------------------------------------------------------------------------ */
 
 int orc_run(int kernel, const int dims[3], const int periodic[3], const int *lattice,
@@ -537,10 +558,11 @@ int orc_run(int kernel, const int dims[3], const int periodic[3], const int *lat
 		s.f = (double *)calloc((size_t)Q * s.gx * s.gy * s.gz, sizeof(double));
 		aa_build_fixup(&s, lattice, periodic);
 	} else {
-		if (list_build(&s.L, kernel == ORC_KERNEL_LIST_PULL, dims, periodic, lattice, blk, pad_mode, 0, NULL, NULL))
+		const int pull = kernel == ORC_KERNEL_LIST_PULL ? 1 : (kernel == ORC_KERNEL_LIST_PULL2 ? 2 : 0);
+		if (list_build(&s.L, pull, dims, periodic, lattice, blk, pad_mode, 0, NULL, NULL))
 			return -1;
 		s.f = (double *)calloc((size_t)Q * s.L.nCells, sizeof(double));
-		if (kernel == ORC_KERNEL_LIST_PULL)
+		if (kernel != ORC_KERNEL_LIST_AA)
 			s.g = (double *)calloc((size_t)Q * s.L.nCells, sizeof(double));
 	}
 
@@ -579,7 +601,10 @@ int orc_run(int kernel, const int dims[3], const int periodic[3], const int *lat
 		}
 	} else {
 		for (int it = 0; it < iterations; ++it) {
-			list_pull(&s, &t);
+			if (kernel == ORC_KERNEL_LIST_PUSH2)
+				list_push2(&s, &t);
+			else
+				list_pull(&s, &t);
 			double *tmp = s.f; s.f = s.g; s.g = tmp;
 			add_body_force(&s, lattice, xforce);
 		}

@@ -28,7 +28,13 @@ extern "C" {
 enum { ORC_GEO_BOX = 0, ORC_GEO_CHANNEL = 1, ORC_GEO_PIPE = 2, ORC_GEO_BLOCKS = 3, ORC_GEO_FLUID = 4 };
 
 /* kernels restated */
-enum { ORC_KERNEL_AA = 0, ORC_KERNEL_LIST_AA = 1, ORC_KERNEL_LIST_PULL = 2 };
+/* LIST_PULL is the pull-split layout (padding plus the cache-line pad of
+ * src/BenchKernelD3Q19ListPullSplitNtCommon.c:494-496); LIST_PUSH2 and
+ * LIST_PULL2 are the two-grid list kernels list-push-soa / list-pull-soa
+ * (src/BenchKernelD3Q19List.c, layout src/BenchKernelD3Q19ListCommon.c:330-600,
+ * padding only). */
+enum { ORC_KERNEL_AA = 0, ORC_KERNEL_LIST_AA = 1, ORC_KERNEL_LIST_PULL = 2, ORC_KERNEL_LIST_PUSH2 = 3,
+       ORC_KERNEL_LIST_PULL2 = 4 };
 
 /* init modes */
 enum { ORC_INIT_ZERO = 0, ORC_INIT_VERIFY = 1, ORC_INIT_PDFS = 2 };

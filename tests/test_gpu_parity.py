@@ -19,7 +19,15 @@ pytestmark = pytest.mark.gpu
 KERNELS = [("cuda-aa-soa", "aa", "aa-soa"),
            ("cuda-list-aa-pv-soa", "list-aa", "list-aa-pv-soa"),
            ("cuda-list-pull-split-nt-1s-soa", "list-pull", "list-pull-split-nt-1s-soa"),
-           ("cuda-list-pull-split-nt-2s-soa", "list-pull", "list-pull-split-nt-2s-soa")]
+           ("cuda-list-pull-split-nt-2s-soa", "list-pull", "list-pull-split-nt-2s-soa"),
+           ("cuda-list-aa-soa", "list-aa", "list-aa-soa"),
+           ("cuda-list-aa-ria-soa", "list-aa", "list-aa-ria-soa"),
+           ("cuda-list-push-soa", "list-push2", "list-push-soa"),
+           ("cuda-list-pull-soa", "list-pull2", "list-pull-soa")]
+
+# reference kernels whose arithmetic is the scalar order (bit-identical to the
+# oracle); the others sum in SIMD order
+SCALAR_REFERENCE = {"aa-soa", "list-aa-soa", "list-aa-ria-soa", "list-push-soa", "list-pull-soa"}
 
 EDGE_CASES = [
     ("fluid", (3, 3, 3), (1, 1, 1)),
@@ -80,7 +88,7 @@ def test_fields_against_reference(reference, kname, okernel, rkernel):
     r = reference.run(rkernel, dims, lat.periodic, lat.mask, omega=1.1, xforce=1e-4, iterations=30,
                       init="pdfs", init_pdfs=init)
     m = lat.mask != 0
-    if rkernel == "aa-soa":
+    if rkernel in SCALAR_REFERENCE:
         assert np.array_equal(g[m], r[m])
     else:
         assert np.max(np.abs(g[m] - r[m]) / np.abs(r[m])) < 1e-13
@@ -144,7 +152,8 @@ def test_channel_64_developed_poiseuille_known_answer(kname):
 
 def test_list_layout_on_device_instance(oracle):
     lat = lbmb200.geometry("pipe", (10, 12, 11), (0, 0, 0))
-    for kname, pull in [("cuda-list-aa-pv-soa", 0), ("cuda-list-pull-split-nt-1s-soa", 1)]:
+    for kname, pull in [("cuda-list-aa-pv-soa", 0), ("cuda-list-pull-split-nt-1s-soa", 1),
+                        ("cuda-list-push-soa", 0), ("cuda-list-pull-soa", 2)]:
         inst = lbmb200.kernel(kname).init(lat)
         try:
             g1, a1, nf1, nc1 = inst.list_layout()

@@ -102,11 +102,29 @@ def test_pad_cells_known_values(oracle):
     assert oracle.pad_cells(1000, pad_mode=1) == 1000
 
 
+@pytest.mark.parametrize("kernel,pull", [("list-push-soa", 0), ("list-pull-soa", 2), ("list-aa-soa", 0),
+                                         ("list-aa-ria-soa", 0)])
+@pytest.mark.parametrize("geo,dims,per,kargs", LAYOUT_CASES[:4])
+def test_other_list_layouts_match_reference(oracle, reference, kernel, pull, geo, dims, per, kargs):
+    # the two-grid list kernels and the other list-AA variants share the
+    # numbering and adjacency rules; two-grid pull has no cache-line pad
+    lat, _ = reference.geometry(geo, dims, per)
+    blk, pad = _kargs_to_oracle(kargs)
+    g1, a1, nf1, nc1 = reference.list_layout(kernel, dims, per, lat, kargs)
+    g2, a2, nf2, nc2 = oracle.list_layout(pull, dims, per, lat, blk, pad)
+    assert (nf1, nc1) == (nf2, nc2)
+    assert np.array_equal(g1, g2) and np.array_equal(a1, a2)
+
+
 @pytest.mark.parametrize("kernel,okernel,exact", [
     ("aa-soa", "aa", True),
     ("list-pull-split-nt-1s-soa", "list-pull", False),
     ("list-pull-split-nt-2s-soa", "list-pull", False),
     ("list-aa-pv-soa", "list-aa", False),
+    ("list-aa-soa", "list-aa", True),
+    ("list-aa-ria-soa", "list-aa", True),
+    ("list-push-soa", "list-push2", True),
+    ("list-pull-soa", "list-pull2", True),
 ])
 @pytest.mark.parametrize("geo,dims,per", FIELD_CASES)
 def test_fields_match_reference(oracle, reference, kernel, okernel, exact, geo, dims, per):
@@ -124,7 +142,7 @@ def test_fields_match_reference(oracle, reference, kernel, okernel, exact, geo, 
         assert np.max(np.abs(r[m] - o[m]) / np.abs(r[m])) < 1e-13
 
 
-@pytest.mark.parametrize("okernel", ["aa", "list-aa", "list-pull"])
+@pytest.mark.parametrize("okernel", ["aa", "list-aa", "list-pull", "list-push2", "list-pull2"])
 def test_verify_known_answer_lambda_1_12(oracle, okernel):
     # reference -verify (16^3 box, periodic x/y, 1000 steps): 4.561374e-02
     dims, per = (16, 16, 16), (1, 1, 0)
@@ -133,7 +151,7 @@ def test_verify_known_answer_lambda_1_12(oracle, okernel):
     assert "%e" % oracle.verify_error(dims, lat, f) == "4.561374e-02"
 
 
-@pytest.mark.parametrize("okernel", ["aa", "list-aa", "list-pull"])
+@pytest.mark.parametrize("okernel", ["aa", "list-aa", "list-pull", "list-push2", "list-pull2"])
 def test_verify_known_answer_lambda_3_16(oracle, okernel):
     # reference with Lambda = 3/16 at the -verify preset: 7.855978e-02
     dims, per = (16, 16, 16), (1, 1, 0)
