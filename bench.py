@@ -184,7 +184,7 @@ def time_kernel(lbmb200, kname, lat, steps, warmup, kargs, dist, odd_key):
         n_launch = inst.last_launches
         per = list(per)[:n_launch]
         res = {"ms": tot.value, "launches": n_launch,
-               "steps_run": steps if "pull" in kname else 2 * pairs,
+               "steps_run": steps if ("pull" in kname or "push" in kname) else 2 * pairs,
                "per_launch_ms": per, "inst": inst,
                "launches_per_pair": inst.launches_for(2)}
         return res
@@ -495,6 +495,14 @@ def run_ours(args, dist):
             "mflups": round(lat.n_fluid / (pm / 1e3) / 1e6, 1), "launch_ms": round(pm, 5),
             "achieved_gbs": round(B_PER_FLUP["pull"] * lat.n_fluid / (pm / 1e3) / 1e9, 1),
             "frac": round(B_PER_FLUP["pull"] * lat.n_fluid / (pm / 1e3) / 1e9 / peak, 4)}
+        # the two-grid list rows on the same domain (376 B per node update)
+        for kname in ("cuda-list-push-soa", "cuda-list-pull-soa"):
+            tq = time_kernel(lbmb200, kname, lat, min(args.steps, 200), 3, kargs, dist, "pull")
+            tq["inst"].deinit()
+            qm = statistics.mean(tq["per_launch_ms"])
+            extra[kname] = {"mflups": round(lat.n_fluid / (qm / 1e3) / 1e6, 1), "launch_ms": round(qm, 5),
+                            "achieved_gbs": round(B_PER_FLUP["pull"] * lat.n_fluid / (qm / 1e3) / 1e9, 1),
+                            "frac": round(B_PER_FLUP["pull"] * lat.n_fluid / (qm / 1e3) / 1e9 / peak, 4)}
         # full-array AA at 256^3: the reference's -geometry fluid with -periodic-x -periodic-y
         # -periodic-z, and -geometry channel (x periodic, walls in y and z)
         for key, geo, per_flags in (("cuda-aa-soa", "fluid", (1, 1, 1)), ("cuda-aa-soa/channel", "channel", (0, 0, 0))):

@@ -240,6 +240,31 @@ int lbm_b200_time_steps(KernelData *kd, CaseData *cd, int n, double *total_ms, d
  * reversed links; face shell), list AA 2 per pair, pull 1 per step. */
 long lbm_b200_launches_for(KernelData *kd, int n);
 
+/* ---- x-slabs of a full-array AA lattice (one lattice over several GPUs) ----
+ * lbm_aa_slab_init: an AA instance (the cuda-aa-soa kernels, Parameters as
+ * its Init) over the x range [x0, x1) of `global`, in local coordinates
+ * (local x = x - x0; GetNode/SetNode/get_field use a LatticeDesc of the slab).
+ * Link words come from the whole lattice, so a link into a neighbouring slab
+ * is direct exactly when the global neighbour is fluid. haloLo / haloHi: the
+ * x = x0 / x = x1-1 face borders a neighbour slab (on the lattice's own x
+ * boundary only with periodic x: the ring's wrap). Returns NULL on errors
+ * (lbm_b200_last_error).
+ * A step pair is: lbm_aa_slab_step(half 0, even step) on every slab; for
+ * every halo face, lbm_aa_halo_pack(side, 0) -> send to the neighbour ->
+ * lbm_aa_halo_unpack(side, 0) there; lbm_aa_slab_step(half 1, odd step); the
+ * same exchange with phase 1. side 0 is the x0 face, 1 the x1-1 face; a
+ * message is lbm_aa_halo_count doubles (5 directions x nY x nZ) in device
+ * memory. Pack of (side 1, phase p) pairs with unpack of (side 0, phase p) on
+ * the right-hand neighbour and vice versa. The functions enqueue on `stream`
+ * (NULL: the instance's stream) and return 0 or an error code; after steps on
+ * another stream, synchronise it before lbm_b200_sync_mirror. */
+KernelData *lbm_aa_slab_init(LatticeDesc *global, int x0, int x1, int haloLo, int haloHi, Parameters *params);
+void lbm_aa_slab_deinit(KernelData *kd);
+long long lbm_aa_halo_count(KernelData *kd);
+int lbm_aa_halo_pack(KernelData *kd, int side, int phase, double *buf, void *stream);
+int lbm_aa_halo_unpack(KernelData *kd, int side, int phase, const double *buf, void *stream);
+int lbm_aa_slab_step(KernelData *kd, CaseData *cd, int half, void *stream);
+
 /* Runs a kernel that waits, with a bound of `polls` reads, on a device flag
  * that nothing sets: the wait runs out, the kernel records error bit 2 in its
  * error word and returns, and *status receives the word (2). The same bounded

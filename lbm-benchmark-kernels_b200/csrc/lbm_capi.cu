@@ -66,6 +66,9 @@ struct Gpu {
   long long dstride;
   int* dOddBlocks;         // interior blocks of the odd step: nDirect direct, then nGeneral general
   int nDirect, nGeneral;
+  // x-slab of a larger lattice (lbm_aa_slab_init): halo/cross flags of the two x faces
+  int halo[2], cross[2];
+  int* sliceMask;          // the slab's own mask (owned)
 
   // list layout
   uint32_t* grid;
@@ -261,6 +264,10 @@ lbm::AaArgs aa_args(Gpu* g) {
   a.perX = g->per[0];
   a.perY = g->per[1];
   a.perZ = g->per[2];
+  a.haloLo = g->halo[0];
+  a.haloHi = g->halo[1];
+  a.crossLo = g->cross[0];
+  a.crossHi = g->cross[1];
   const int S = (int)g->dstride;
   for (int d = 0; d < Q; ++d) {
     const int j = lbm::inv(d);
@@ -493,7 +500,14 @@ void cb_kernel(LatticeDesc* ld, KernelData* kd, CaseData* cd) {
 
 // --- Init / Deinit ----------------------------------------------------------------
 
-Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params) {
+// The x range [x0, x1) of a larger lattice that an AA instance covers.
+struct SlabSpec {
+  const LatticeDesc* global;
+  int x0, x1;
+  int halo[2];
+};
+
+Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* slab = nullptr) {
   Gpu* g = static_cast<Gpu*>(std::calloc(1, sizeof(Gpu)));
   if (!g) { std::printf("ERROR: allocation failed.\n"); std::exit(1); }
   Args a = parse_args(params);
@@ -552,7 +566,15 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params) {
 
     uint32_t* link = static_cast<uint32_t*>(std::malloc(sizeof(uint32_t) * (size_t)g->dstride));
     if (!link) { std::printf("ERROR: allocation failed.\n"); std::exit(1); }
-    lbmh_aa_links(ld, g->xs, g->pitch, lbm::kZOff, link);
+    if (slab) {
+      lbmh_aa_links_range(slab->global, slab->x0, slab->x1, g->xs, g->pitch, lbm::kZOff, link);
+      for (int s2 = 0; s2 < 2; ++s2) g->halo[s2] = slab->halo[s2];
+      // a halo face on the lattice's own x boundary is its periodic wrap
+      g->cross[0] = slab->halo[0] && slab->x0 == 0;
+      g->cross[1] = slab->halo[1] && slab->x1 == slab->global->Dims[0];
+    } else {
+      lbmh_aa_links(ld, g->xs, g->pitch, lbm::kZOff, link);
+    }
     LBM_CK(cudaMalloc(&g->dLink, sizeof(uint32_t) * (size_t)g->dstride));
     LBM_CK(cudaMemcpy(g->dLink, link, sizeof(uint32_t) * (size_t)g->dstride, cudaMemcpyHostToDevice));
     LBM_CK(cudaMalloc(&g->dF, sizeof(double) * g->mirrorElems));
@@ -645,6 +667,7 @@ void gpu_free(KernelData** kernelData) {
   cudaFree(g->dG);
   cudaFree(g->dLink);
   cudaFree(g->dOddBlocks);
+  std::free(g->sliceMask);
   cudaFree(g->dAdj);
   cudaFree(g->dErr);
   cudaFree(g->dMomOut);
@@ -814,6 +837,97 @@ int lbm_b200_sync_mirror(KernelData* kd) {
 const char* lbm_b200_last_error(void) { return g_lastError.c_str(); }
 
 long lbm_b200_launches_for(KernelData* kd, int n) { return launches_for(reinterpret_cast<Gpu*>(kd), n); }
+
+// --- x-slabs of a full-array AA lattice ----------------------------------------
+
+KernelData* lbm_aa_slab_init(LatticeDesc* global, int x0, int x1, int haloLo, int haloHi, Parameters* params) {
+  const int nx = global->Dims[0], ny = global->Dims[1], nz = global->Dims[2];
+  if (x0 < 0 || x1 > nx || x1 - x0 < 1) {
+    g_lastError = "slab range outside the lattice";
+    return nullptr;
+  }
+  if ((haloLo || haloHi) && global->PeriodicX == 0 && ((haloLo && x0 == 0) || (haloHi && x1 == nx))) {
+    g_lastError = "a halo face on the lattice's x boundary needs a periodic x axis";
+    return nullptr;
+  }
+  const int L = x1 - x0;
+  int* mask = static_cast<int*>(std::malloc(sizeof(int) * (size_t)L * ny * nz));
+  if (!mask) return nullptr;
+  int nFluid = 0;
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < L; ++x) {
+        const int v = global->Lattice[((long)z * ny + y) * nx + x0 + x];
+        mask[((long)z * ny + y) * L + x] = v;
+        nFluid += v != LAT_CELL_OBSTACLE;
+      }
+  LatticeDesc local = *global;
+  local.Dims[0] = L;
+  local.Lattice = mask;
+  local.nCells = L * ny * nz;
+  local.nFluid = nFluid;
+  local.nObst = local.nCells - nFluid;
+  SlabSpec spec{global, x0, x1, {haloLo != 0, haloHi != 0}};
+  Gpu* g = gpu_new(kAa, &local, params, &spec);
+  g->sliceMask = mask;
+  return &g->kd;
+}
+
+void lbm_aa_slab_deinit(KernelData* kd) {
+  KernelData* k = kd;
+  gpu_free(&k);
+}
+
+long long lbm_aa_halo_count(KernelData* kd) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  return 5LL * g->dims[1] * g->dims[2];
+}
+
+// Pending SetNode edits go up on the instance's stream, which is then
+// drained: the caller's stream may be another one.
+static void sync_upload(Gpu* g) {
+  if (!g->dirty) return;
+  upload_if_dirty(g);
+  LBM_CK(cudaStreamSynchronize(g->stream));
+}
+
+static cudaStream_t stream_or(Gpu* g, void* stream) {
+  return stream ? static_cast<cudaStream_t>(stream) : g->stream;
+}
+
+int lbm_aa_halo_pack(KernelData* kd, int side, int phase, double* buf, void* stream) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (g->kind != kAa || side < 0 || side > 1 || phase < 0 || phase > 1) return -1;
+  sync_upload(g);
+  lbm::aa_halo_pack(aa_args(g), side, phase, buf, stream_or(g, stream));
+  return (int)cudaGetLastError();
+}
+
+int lbm_aa_halo_unpack(KernelData* kd, int side, int phase, const double* buf, void* stream) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (g->kind != kAa || side < 0 || side > 1 || phase < 0 || phase > 1) return -1;
+  sync_upload(g);
+  lbm::aa_halo_unpack(aa_args(g), side, phase, buf, stream_or(g, stream));
+  return (int)cudaGetLastError();
+}
+
+int lbm_aa_slab_step(KernelData* kd, CaseData* cd, int half, void* stream) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (g->kind != kAa || half < 0 || half > 1) return -1;
+  sync_upload(g);
+  const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
+  const lbm::AaArgs a = aa_args(g);
+  const cudaStream_t s = stream_or(g, stream);
+  if (half == 0) {
+    lbm::aa_even_fp64(a, t, s);
+  } else {
+    if (g->nDirect > 0) lbm::aa_odd_interior_fp64(a, t, g->dOddBlocks, g->nDirect, 0, s);
+    if (g->nGeneral > 0) lbm::aa_odd_interior_fp64(a, t, g->dOddBlocks + g->nDirect, 0, g->nGeneral, s);
+    if (lbm::aa_shell_cells(a) > 0) lbm::aa_odd_face_fp64(a, t, s);
+    g->iteration += 2;
+  }
+  return (int)cudaGetLastError();
+}
 
 int lbm_b200_checkpoint_save(KernelData* kd, const char* path) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);

@@ -253,13 +253,22 @@ int lbmh_list_build(const LatticeDesc *ld, int pull, const int blk[3], int nCell
 
 void lbmh_aa_links(const LatticeDesc *ld, int xs, int pitch, int zoff, uint32_t *link)
 {
+	lbmh_aa_links_range(ld, 0, ld->Dims[0], xs, pitch, zoff, link);
+}
+
+/* The link words of the x-slab [x0, x1) of the lattice ld, in the slab's own
+ * full-array layout (local x = global x - x0): the classification uses the
+ * whole lattice, so a link into a neighbouring slab is reversed exactly when
+ * the global neighbour is not a fluid node. */
+void lbmh_aa_links_range(const LatticeDesc *ld, int x0, int x1, int xs, int pitch, int zoff, uint32_t *link)
+{
 	const int *dims = ld->Dims;
-	const int nx = dims[0], ny = dims[1], nz = dims[2];
+	const int ny = dims[1], nz = dims[2];
 	const int per[3] = { ld->PeriodicX, ld->PeriodicY, ld->PeriodicZ };
-	const long total = (long)(nx + 2) * xs;
+	const long total = (long)(x1 - x0 + 2) * xs;
 	memset(link, 0, sizeof(uint32_t) * (size_t)total);
 
-	for (int x = 0; x < nx; ++x) for (int y = 0; y < ny; ++y) for (int z = 0; z < nz; ++z) {
+	for (int x = x0; x < x1; ++x) for (int y = 0; y < ny; ++y) for (int z = 0; z < nz; ++z) {
 		if (ld->Lattice[lbmh_lidx(dims, x, y, z)] == LAT_CELL_OBSTACLE) continue;
 		uint32_t w = 0x80000000u;
 		for (int d = 0; d < 18; ++d) {
@@ -283,7 +292,7 @@ void lbmh_aa_links(const LatticeDesc *ld, int xs, int pitch, int zoff, uint32_t 
 			}
 			if (reversed) w |= 1u << d;
 		}
-		link[(long)(x + 1) * xs + (long)(y + 1) * pitch + z + zoff] = w;
+		link[(long)(x - x0 + 1) * xs + (long)(y + 1) * pitch + z + zoff] = w;
 	}
 }
 

@@ -38,6 +38,7 @@ int lbmh_list_build(const LatticeDesc *ld, int pull, const int blk[3], int nCell
  * cell does not reach a fluid node (wall or open face). Ghost and pad cells
  * get 0. cellOf(x,y,z) = (x+1)*xs + (y+1)*pitch + z + zoff. */
 void lbmh_aa_links(const LatticeDesc *ld, int xs, int pitch, int zoff, uint32_t *link);
+void lbmh_aa_links_range(const LatticeDesc *ld, int x0, int x1, int xs, int pitch, int zoff, uint32_t *link);
 
 /* IEEE binary16 <-> binary32 (round to nearest even). */
 float lbmh_f16_to_f32(uint16_t h);

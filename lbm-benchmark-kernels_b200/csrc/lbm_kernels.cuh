@@ -39,7 +39,22 @@ struct AaArgs {
   // the parameter bank: the odd step's load of d (slot inv(d) of x + c_inv(d))
   // and store of d (slot d of x + c_d); the centre uses its own slot
   int ldOff[Q], stOff[Q];
+  // x-slab of a larger lattice: a halo face (haloLo at x = 0, haloHi at
+  // x = nX-1) borders the neighbouring slab, whose face plane the ghost plane
+  // mirrors (exchanged around the odd step); cross* marks a halo face that is
+  // also the lattice's periodic x boundary. All 0 for a whole lattice.
+  int haloLo, haloHi, crossLo, crossHi;
 };
+
+// x-slab halo exchange (lbm_kernels_fp64.cu). A message is the 5 PDFs that
+// cross one x face, over the face's nY x nZ cells: [k][y][z]. side 0 = the
+// x = 0 face, 1 = the x = nX-1 face. Phase 0 (after the even step): pack the
+// face plane's slots that the neighbour's cells read and write in the odd
+// step / unpack them into the ghost plane. Phase 1 (after the odd step): pack
+// the ghost plane's slots this slab's cells wrote / unpack them into the face
+// plane.
+void aa_halo_pack(const AaArgs& a, int side, int phase, double* buf, cudaStream_t s);
+void aa_halo_unpack(const AaArgs& a, int side, int phase, const double* buf, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // Fluid-node list layout (the reference's list kernels).

@@ -45,7 +45,8 @@ __device__ __forceinline__ int aa_off(const AaArgs& a, int d) { return cx(d) * a
 // reach a fluid node, i.e. in-range or periodic ones.
 __device__ __forceinline__ int aa_wrapped(const AaArgs& a, int x, int y, int z, int d) {
   int nx = x + cx(d), ny = y + cy(d), nz = z + cz(d);
-  nx = nx < 0 ? a.nX - 1 : (nx >= a.nX ? 0 : nx);
+  // across a halo face the neighbour slab's cell is mirrored in the ghost plane
+  nx = nx < 0 ? (a.haloLo ? -1 : a.nX - 1) : (nx >= a.nX ? (a.haloHi ? a.nX : 0) : nx);
   ny = ny < 0 ? a.nY - 1 : (ny >= a.nY ? 0 : ny);
   nz = nz < 0 ? a.nZ - 1 : (nz >= a.nZ ? 0 : nz);
   return aa_cell(a, nx, ny, nz);
@@ -56,7 +57,9 @@ __device__ __forceinline__ int aa_wrapped(const AaArgs& a, int x, int y, int z, 
 // reference, instead of bouncing back.
 __device__ __forceinline__ bool aa_open(const AaArgs& a, int x, int y, int z, int d) {
   int nx = x + cx(d), ny = y + cy(d), nz = z + cz(d);
-  bool ox = nx < 0 || nx >= a.nX, oy = ny < 0 || ny >= a.nY, oz = nz < 0 || nz >= a.nZ;
+  // crossing a halo face leaves the lattice only where it is the periodic x boundary
+  bool ox = (nx < 0 && (!a.haloLo || a.crossLo)) || (nx >= a.nX && (!a.haloHi || a.crossHi));
+  bool oy = ny < 0 || ny >= a.nY, oz = nz < 0 || nz >= a.nZ;
   bool crossesPeriodic = (ox && a.perX) || (oy && a.perY) || (oz && a.perZ);
   return (ox || oy || oz) && !crossesPeriodic;
 }
@@ -220,6 +223,51 @@ __global__ void __launch_bounds__(128) k_aa_odd_face_fp64(const AaArgs a, const 
     }
   };
   trt_update(t, load, store);
+}
+
+// ---------------------------------------------------------------------------
+// x-slab halo messages.
+
+// The 5 directions with c_x = +1 (E, NE, SE, TE, BE) and c_x = -1 (W, NW, SW,
+// TW, BW), in the order of a message.
+__device__ __forceinline__ int halo_dir(int k, bool plusX) {
+  return plusX ? (k == 0 ? E : k == 1 ? NE : k == 2 ? SE : k == 3 ? TE : BE)
+               : (k == 0 ? W : k == 1 ? NW : k == 2 ? SW : k == 3 ? TW : BW);
+}
+
+// plane: local x of the plane (-1 and nX are the ghost planes); plusX: which
+// five directions; toBuf: copy the slots into buf, else out of it.
+__global__ void k_aa_halo(const AaArgs a, int plane, bool plusX, bool toBuf, double* buf) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long face = (long long)a.nY * a.nZ;
+  if (i >= 5 * face) return;
+  const int k = (int)(i / face);
+  const int y = (int)(i % face / a.nZ), z = (int)(i % a.nZ);
+  const long long slot = halo_dir(k, plusX) * a.dstride + (long long)(plane + 1) * a.xs +
+                         (long long)(y + 1) * a.pitch + z + kZOff;
+  if (toBuf)
+    buf[i] = a.f[slot];
+  else
+    a.f[slot] = buf[i];
+}
+
+// Side 1 (x = nX-1 face): the cells of this slab cross it with c_x = +1, the
+// neighbour's with c_x = -1; side 0 the other way round.
+void aa_halo_pack(const AaArgs& a, int side, int phase, double* buf, cudaStream_t s) {
+  const long long n = 5LL * a.nY * a.nZ;
+  const int plane = phase == 0 ? (side == 0 ? 0 : a.nX - 1) : (side == 0 ? -1 : a.nX);
+  // phase 0: the face plane's slots the neighbour streams through (pointing
+  // into this slab); phase 1: the ghost plane's slots this slab streamed into
+  const bool plusX = phase == 0 ? side == 0 : side == 1;
+  if (n > 0) k_aa_halo<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, plane, plusX, true, buf);
+}
+
+void aa_halo_unpack(const AaArgs& a, int side, int phase, const double* buf, cudaStream_t s) {
+  const long long n = 5LL * a.nY * a.nZ;
+  const int plane = phase == 0 ? (side == 0 ? -1 : a.nX) : (side == 0 ? 0 : a.nX - 1);
+  const bool plusX = phase == 0 ? side == 1 : side == 0;
+  if (n > 0)
+    k_aa_halo<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, plane, plusX, false, const_cast<double*>(buf));
 }
 
 long long aa_shell_cells(const AaArgs& a) {

@@ -1,0 +1,68 @@
+"""Command-line run of one full-array AA lattice split into x-slabs, one slab
+per GPU, halo messages through torch.distributed (NCCL):
+
+    python -m torch.distributed.run --nproc-per-node 4 --master-addr 127.0.0.1 \\
+        -m lbmb200.slabrun --dims 1024x256x256 --geometry fluid --periodic xyz --pairs 50
+
+(run with lbm-benchmark-kernels_b200 on the Python path). Every rank builds the
+same lattice, takes its slab, and runs `pairs` even/odd step pairs; rank 0
+prints the aggregate MFLUP/s (device-timed per rank with CUDA events, max over
+ranks). With one process, the lattice runs as one slab without halos.
+"""
+import argparse
+import json
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    p.add_argument("--dims", default="256x256x256")
+    p.add_argument("--geometry", default="fluid")
+    p.add_argument("--periodic", default="xyz", help="periodic axes, e.g. xyz or x")
+    p.add_argument("--pairs", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--omega", type=float, default=1.0)
+    p.add_argument("--lambda", dest="lam", default="3/16")
+    a = p.parse_args(argv)
+
+    import torch
+    import torch.distributed as dist
+
+    import lbmb200
+    from lbmb200 import slabs as sl
+    from lbmb200.ranks import Ranks
+
+    ranks = Ranks()
+    try:
+        dims = tuple(int(v) for v in a.dims.split("x"))
+        per = tuple(int(c in a.periodic) for c in "xyz")
+        lat = lbmb200.geometry(a.geometry, dims, per)
+        x0, x1 = sl.partition(dims[0], ranks.world)[ranks.rank]
+        lo, hi = sl.halo_flags(ranks.rank, ranks.world, lat.periodic[0])
+        lbmb200.lib().lbm_b200_set_device(ranks.local)
+        torch.cuda.set_device(ranks.local)
+        slab = sl.Slab(lat, x0, x1, lo, hi, kernel_args=["-lambda", a.lam])
+        stream = torch.cuda.current_stream().cuda_stream
+        tr = sl.DistTransport(slab, ranks.rank, ranks.world, lat.periodic[0], dist,
+                              lambda n: torch.empty(n, dtype=torch.float64, device="cuda"), stream=stream)
+        cd = lbmb200.case(omega=a.omega, xforce=1e-5)
+        sl.step_pairs([slab], tr, cd, a.warmup, stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ranks.barrier()
+        e0.record()
+        sl.step_pairs([slab], tr, cd, a.pairs, stream)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = ranks.max(e0.elapsed_time(e1))
+        nodes = ranks.sum(slab.local.n_fluid)
+        if ranks.rank == 0:
+            print(json.dumps({"dims": dims, "geometry": a.geometry, "ranks": ranks.world, "fluid_nodes": nodes,
+                              "pairs": a.pairs, "ms": round(ms, 3),
+                              "mflups": round(nodes * 2 * a.pairs / (ms / 1e3) / 1e6, 1)}))
+        slab.close()
+    finally:
+        ranks.close()
+
+
+if __name__ == "__main__":
+    main()

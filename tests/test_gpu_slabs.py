@@ -1,0 +1,74 @@
+"""One full-array AA lattice split into x-slabs (lbm_aa_slab_*, lbmb200.slabs):
+slabs in one process on one GPU, halo messages through device buffers on one
+stream, against the single-instance kernel -- bit for bit after every pair.
+(With one slab per GPU the messages travel through torch.distributed instead;
+that transport's pairing is tested on CPU ranks in test_slabs_gloo.py.)"""
+import numpy as np
+import pytest
+
+import lbmb200
+from lbm_cases import random_pdfs
+from lbmb200 import slabs as sl
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    ("fluid", (24, 10, 12), (1, 1, 1), 2),
+    ("fluid", (25, 9, 11), (1, 1, 1), 3),    # uneven slabs, periodic ring
+    ("fluid", (9, 8, 7), (1, 0, 1), 4),      # thin slabs, corner links wrap on several axes
+    ("fluid", (6, 7, 8), (1, 1, 0), 3),      # two-plane slabs, open z faces
+    ("channel", (30, 12, 14), (0, 0, 0), 3), # closed x faces on the end slabs
+    ("box", (20, 10, 12), (0, 1, 1), 2),
+    ("blocks-2", (26, 11, 12), (1, 0, 1), 3),
+    ("fluid", (9, 8, 7), (0, 0, 0), 2),      # all faces open
+]
+
+
+def _run_slabs(lat, parts, init, cd, pairs):
+    import torch
+    stream = torch.cuda.current_stream().cuda_stream
+    ranges = sl.partition(lat.dims[0], parts)
+    slabs = [sl.Slab(lat, x0, x1, *sl.halo_flags(r, parts, lat.periodic[0]), kernel_args=["-lambda", "3/16"])
+             for r, (x0, x1) in enumerate(ranges)]
+    try:
+        sl.scatter_field(slabs, lat, init)
+        tr = sl.LocalTransport(slabs, lat.periodic[0], stream,
+                               lambda n: torch.empty(n, dtype=torch.float64, device="cuda"))
+        sl.step_pairs(slabs, tr, cd, pairs, stream)
+        torch.cuda.synchronize()
+        return sl.gather_field(slabs, lat)
+    finally:
+        for s in slabs:
+            s.close()
+
+
+@pytest.mark.parametrize("geo,dims,per,parts", CASES)
+def test_slabs_equal_whole_lattice(geo, dims, per, parts):
+    lat = lbmb200.geometry(geo, dims, per)
+    init = random_pdfs(lat.mask.size, 31)
+    cd = lbmb200.case(omega=1.2, xforce=2e-4, iterations=10)
+    inst = lbmb200.kernel("cuda-aa-soa").init(lat, kernel_args=["-lambda", "3/16"])
+    try:
+        inst.set_field(init)
+        inst.run(cd)
+        whole = inst.get_field()
+    finally:
+        inst.deinit()
+    got = _run_slabs(lat, parts, init, cd, 5)
+    m = lat.mask != 0
+    assert np.array_equal(got[m], whole[m])
+
+
+def test_slab_refuses_halo_on_closed_boundary():
+    lat = lbmb200.geometry("channel", (12, 8, 8), (0, 0, 0))
+    with pytest.raises(RuntimeError, match="periodic"):
+        sl.Slab(lat, 0, 6, True, True)
+
+
+def test_slabrun_single_process(capsys):
+    from lbmb200 import slabrun
+    slabrun.main(["--dims", "32x16x16", "--pairs", "2", "--warmup", "1"])
+    out = capsys.readouterr().out.strip().splitlines()[-1]
+    import json
+    rec = json.loads(out)
+    assert rec["ranks"] == 1 and rec["fluid_nodes"] == 32 * 16 * 16 and rec["mflups"] > 0
