@@ -149,6 +149,18 @@ void D3Q19CudaListDeinit_PushSoA(LatticeDesc *ld, KernelData **kernelData);
 void D3Q19CudaListInit_PullSoA(LatticeDesc *ld, KernelData **kernelData, Parameters *params);
 void D3Q19CudaListDeinit_PullSoA(LatticeDesc *ld, KernelData **kernelData);
 
+/* "cuda-push-soa" / "cuda-pull-soa": the two-grid full-array kernels
+ * (src/BenchKernelD3Q19.c, registered at src/KernelFunctions.h:126-145 as
+ * D3Q19Init_PushSoA / D3Q19Init_PullSoA and their Deinit), on the
+ * full-array layout of cuda-aa-soa with a second grid; the reference's
+ * bounce-back/periodic fix-up lists and body-force pass are folded into the
+ * stores. GetNode of pull-soa views node x's PDF d at x - c_d, as the
+ * reference's. */
+void D3Q19CudaInit_PushSoA(LatticeDesc *ld, KernelData **kernelData, Parameters *params);
+void D3Q19CudaDeinit_PushSoA(LatticeDesc *ld, KernelData **kernelData);
+void D3Q19CudaInit_PullSoA(LatticeDesc *ld, KernelData **kernelData, Parameters *params);
+void D3Q19CudaDeinit_PullSoA(LatticeDesc *ld, KernelData **kernelData);
+
 /* The rows above as a table: {Name, Init, Deinit}, in the layout of the
  * reference's KernelFunctions (src/KernelFunctions.h:49-54). */
 typedef struct LbmB200KernelFunctions_ {

@@ -30,9 +30,13 @@ using lbm::QM;
 
 // kListPull: pull-split layout (with its cache-line pad); kListPullPlain and
 // kListPush: the two-grid list kernels list-pull-soa / list-push-soa
-enum Kind { kAa = 0, kListAa = 1, kListPull = 2, kListPullPlain = 3, kListPush = 4 };
+// kFaPush / kFaPull: the two-grid full-array kernels push-soa / pull-soa
+enum Kind { kAa = 0, kListAa = 1, kListPull = 2, kListPullPlain = 3, kListPush = 4, kFaPush = 5, kFaPull = 6 };
 
-bool two_grid(int kind) { return kind == kListPull || kind == kListPullPlain || kind == kListPush; }
+bool full_array(int kind) { return kind == kAa || kind == kFaPush || kind == kFaPull; }
+bool two_grid(int kind) {
+  return kind == kListPull || kind == kListPullPlain || kind == kListPush || kind == kFaPush || kind == kFaPull;
+}
 
 thread_local std::string g_lastError;
 
@@ -201,7 +205,13 @@ double f16_scale_of(int d) { return d == lbm::DC ? 32768.0 : (weight_of(d) > 0.0
 // --- logical node view on the mirror ---------------------------------------
 
 inline double* slot(Gpu* g, int x, int y, int z, int d) {
-  if (g->kind == kAa) {
+  if (full_array(g->kind)) {
+    // pull-soa keeps node x's PDF d at x - c_d (src/BenchKernelD3Q19Common.c:120-196)
+    if (g->kind == kFaPull) {
+      x -= lbm::cx(d);
+      y -= lbm::cy(d);
+      z -= lbm::cz(d);
+    }
     long c = (long)(x + 1) * g->xs + (long)(y + 1) * g->pitch + z + lbm::kZOff;
     return g->mirror + d * g->dstride + c;
   }
@@ -214,7 +224,7 @@ void check_node(Gpu* g, int x, int y, int z) {
     std::printf("ERROR: node (%d, %d, %d) outside the lattice.\n", x, y, z);
     std::exit(1);
   }
-  if (g->kind != kAa && g->grid[lbmh_lidx(g->dims, x, y, z)] == 0xffffffffu) {
+  if (!full_array(g->kind) && g->grid[lbmh_lidx(g->dims, x, y, z)] == 0xffffffffu) {
     std::printf("ERROR: node (%d, %d, %d) is an obstacle and has no PDFs in a list layout.\n", x, y, z);
     std::exit(1);
   }
@@ -253,7 +263,8 @@ void cb_bc_set(KernelData* kd, int x, int y, int z, int dir, PdfT pdf) {
 
 lbm::AaArgs aa_args(Gpu* g) {
   lbm::AaArgs a;
-  a.f = g->dF;
+  a.f = g->cur == 0 ? g->dF : g->dG;  // two-grid kinds: source grid, then
+  a.g = g->cur == 0 ? g->dG : g->dF;  // destination grid (null for AA)
   a.dstride = g->dstride;
   a.link = g->dLink;
   a.nX = g->dims[0];
@@ -355,6 +366,18 @@ long enqueue_steps(Gpu* g, const lbm::Trt<double>& t, int n, cudaEvent_t* ev = n
       lbm::list_odd_fp64(a, t, g->stream);
       ++k;
       g->iteration = it + 1;
+    }
+  } else if (g->kind == kFaPush || g->kind == kFaPull) {
+    for (int it = 0; it < n; ++it) {
+      const lbm::AaArgs a = aa_args(g);
+      mark();
+      if (g->kind == kFaPush)
+        lbm::fa_push_fp64(a, t, g->stream);
+      else
+        lbm::fa_pull_fp64(a, t, g->stream);
+      ++k;
+      g->cur ^= 1;
+      g->iteration = it;
     }
   } else {
     for (int it = 0; it < n; ++it) {
@@ -477,7 +500,8 @@ void cb_kernel(LatticeDesc* ld, KernelData* kd, CaseData* cd) {
     std::printf("ERROR: omega must lie in (0, 2).\n");
     std::exit(1);
   }
-  if (cd->VtkOutput) vtk_or_exit(ld, kd, cd, -1);
+  // the two-grid full-array kernels label their first file 0 (src/BenchKernelD3Q19.c:98-101)
+  if (cd->VtkOutput) vtk_or_exit(ld, kd, cd, (g->kind == kFaPush || g->kind == kFaPull) ? 0 : -1);
   upload_if_dirty(g);
   const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
 
@@ -546,7 +570,7 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* sla
     std::exit(1);
   }
 
-  if (kind == kAa) {
+  if (full_array(kind)) {
     const int gx = ld->Dims[0] + 2, gy = ld->Dims[1] + 2;
     g->pitch = (ld->Dims[2] + lbm::kZOff + 1 + 3) / 4 * 4;
     g->xs = gy * g->pitch;
@@ -579,9 +603,13 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* sla
     LBM_CK(cudaMemcpy(g->dLink, link, sizeof(uint32_t) * (size_t)g->dstride, cudaMemcpyHostToDevice));
     LBM_CK(cudaMalloc(&g->dF, sizeof(double) * g->mirrorElems));
     LBM_CK(cudaMemset(g->dF, 0, sizeof(double) * g->mirrorElems));
-    // the odd step's interior blocks, direct ones first
+    if (kind != kAa) {
+      LBM_CK(cudaMalloc(&g->dG, sizeof(double) * g->mirrorElems));
+      LBM_CK(cudaMemset(g->dG, 0, sizeof(double) * g->mirrorElems));
+    }
+    // the AA odd step's interior blocks, direct ones first
     const lbm::AaArgs aa = aa_args(g);
-    const long long nb = lbm::aa_interior_block_count(aa);
+    const long long nb = kind == kAa ? lbm::aa_interior_block_count(aa) : 0;
     if (nb > 0) {
       int* blocks = static_cast<int*>(std::malloc(sizeof(int) * (size_t)nb));
       if (!blocks) { std::printf("ERROR: allocation failed.\n"); std::exit(1); }
@@ -790,6 +818,21 @@ void D3Q19CudaListDeinit_PullSoA(LatticeDesc* ld, KernelData** kernelData) {
   gpu_free(kernelData);
 }
 
+void D3Q19CudaInit_PushSoA(LatticeDesc* ld, KernelData** kernelData, Parameters* params) {
+  *kernelData = &gpu_new(kFaPush, ld, params)->kd;
+}
+void D3Q19CudaDeinit_PushSoA(LatticeDesc* ld, KernelData** kernelData) {
+  (void)ld;
+  gpu_free(kernelData);
+}
+void D3Q19CudaInit_PullSoA(LatticeDesc* ld, KernelData** kernelData, Parameters* params) {
+  *kernelData = &gpu_new(kFaPull, ld, params)->kd;
+}
+void D3Q19CudaDeinit_PullSoA(LatticeDesc* ld, KernelData** kernelData) {
+  (void)ld;
+  gpu_free(kernelData);
+}
+
 static const LbmB200KernelFunctions kTable[] = {
     {"cuda-aa-soa", D3Q19CudaAaInit_AaSoA, D3Q19CudaAaDeinit_AaSoA},
     {"cuda-list-aa-pv-soa", D3Q19CudaListAaPvInit_PushSoA, D3Q19CudaListAaPvDeinit_PushSoA},
@@ -799,6 +842,8 @@ static const LbmB200KernelFunctions kTable[] = {
     {"cuda-list-aa-ria-soa", D3Q19CudaListAaRiaInit_PushSoA, D3Q19CudaListAaRiaDeinit_PushSoA},
     {"cuda-list-push-soa", D3Q19CudaListInit_PushSoA, D3Q19CudaListDeinit_PushSoA},
     {"cuda-list-pull-soa", D3Q19CudaListInit_PullSoA, D3Q19CudaListDeinit_PullSoA},
+    {"cuda-push-soa", D3Q19CudaInit_PushSoA, D3Q19CudaDeinit_PushSoA},
+    {"cuda-pull-soa", D3Q19CudaInit_PullSoA, D3Q19CudaDeinit_PullSoA},
 };
 
 const LbmB200KernelFunctions* lbm_b200_kernels(int* count) {
@@ -1026,7 +1071,7 @@ int lbm_b200_time_steps(KernelData* kd, CaseData* cd, int n, double* total_ms, d
 
 int lbm_b200_device_state(KernelData* kd, double** pdfs, long long* nCells, int* nFluid, void** stream) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
-  if (g->kind == kAa) return -1;
+  if (full_array(g->kind)) return -1;
   if (pdfs) *pdfs = current_grid(g);
   if (nCells) *nCells = g->nCells;
   if (nFluid) *nFluid = g->nFluid;
@@ -1038,7 +1083,7 @@ int lbm_b200_moments_device(const double* pdfs, long long nCells, int nFluid, do
 
 int lbm_b200_instance_moments(KernelData* kd, double* out) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
-  if (g->kind == kAa || g->storage != lbm::kStoreF64) return -1;
+  if (full_array(g->kind) || g->storage != lbm::kStoreF64) return -1;
   if (g->dirty) upload_if_dirty(g);
   if (g->dMomOut == nullptr) {
     cudaError_t e = cudaMalloc(&g->dMomOut, 4 * sizeof(double));
@@ -1084,7 +1129,7 @@ void lbm_b200_set_field(KernelData* kd, LatticeDesc* ld, const double* in) {
 // grid (nX*nY*nZ), adjacency (nFluid*18, the reference's order), counts.
 int lbm_b200_list_layout(KernelData* kd, const uint32_t** grid, const uint32_t** adj, int* nFluid, int* nCells) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
-  if (g->kind == kAa) return -1;
+  if (full_array(g->kind)) return -1;
   if (adj && !g->adjHost && g->nFluid > 0) {
     // the adjacency lives on the device; a host copy is made on first request
     g->adjHost = static_cast<uint32_t*>(std::malloc(sizeof(uint32_t) * (size_t)g->nFluid * QM));

@@ -30,6 +30,7 @@ constexpr uint32_t kLinkBits = 0x3ffffu;  // the 18 reversed-link bits
 
 struct AaArgs {
   double* f;
+  double* g;  // two-grid full-array kernels: the destination grid (same layout)
   long long dstride;
   const uint32_t* link;
   int nX, nY, nZ;
@@ -118,6 +119,10 @@ long long aa_interior_block_count(const AaArgs& a);
 void aa_interior_blocks(const AaArgs& a, const uint32_t* link, int* blocks, int* nDirect, int* nGeneral);
 void aa_odd_face_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
 bool aa_has_interior(const AaArgs& a);
+// Two-grid full-array push / pull steps (push-soa / pull-soa): every fluid
+// cell from grid a.f into grid a.g.
+void fa_push_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
+void fa_pull_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
 long long aa_shell_cells(const AaArgs& a);
 void list_even_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
 void list_odd_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);

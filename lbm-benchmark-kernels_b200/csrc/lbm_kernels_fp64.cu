@@ -270,6 +270,89 @@ void aa_halo_unpack(const AaArgs& a, int side, int phase, const double* buf, cud
     k_aa_halo<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, plane, plusX, false, const_cast<double*>(buf));
 }
 
+// ---------------------------------------------------------------------------
+// Two-grid full array (src/BenchKernelD3Q19.c:114-344) on the AA layout and
+// link words, one thread per cell, obstacles skipped. The reference's
+// bounce-back and periodic fix-up lists (src/BenchKernelD3Q19Common.c:
+// 531-660), which copy slots after each step, and its body-force pass, which
+// adds 3 w_i c_ix F through the logical node view, are folded into the
+// stores; the result in every slot some fluid node views is the reference's
+// bit for bit (tests against the oracle and the reference).
+
+// Push: node x's own PDFs in from grid f; PDF d out to (x + c_d, d) of grid g
+// (across a periodic face: the wrapped cell). A wall sends it back to the
+// node's own slot inv(d); an open face leaves that slot untouched by the step,
+// so only the force increment is added to what the grid held.
+__global__ void __launch_bounds__(128) k_fa_push_fp64(const AaArgs a, const Trt<double> t) {
+  const int z = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * 4 + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= a.nZ || y >= a.nY) return;
+  const int c = aa_cell(a, x, y, z);
+  const uint32_t w = __ldg(a.link + c);
+  if (!(w & kFluidBit)) return;
+  const long long S = a.dstride;
+  const double* const f = a.f + c;
+  double* const g = launder(a.g);
+  auto store = [&](int d, double v) {
+    if (d == DC) {
+      g[DC * S + c] = v + t.force[DC];
+      return;
+    }
+    const int j = inv(d);
+    if (!((w >> d) & 1u))
+      g[d * S + aa_wrapped(a, x, y, z, d)] = v + t.force[d];
+    else if (aa_open(a, x, y, z, d))
+      g[j * S + c] = g[j * S + c] + t.force[j];
+    else
+      g[j * S + c] = v + t.force[j];
+  };
+  trt_update(t, [&](int d) { return f[d * S]; }, store);
+}
+
+// Pull: PDF d in from (x - c_d, d) of grid f (the slot the previous step
+// filled for this node, ghost cells included); own PDFs out to grid g. For a
+// link e that the next step pulls through a ghost or wall slot, the copy the
+// reference's fix-up list makes is written directly: a wall slot (x + c_e,
+// inv(e)) gets this node's PDF e (bounce back), the ghost slot of the periodic
+// image q = wrap(x + c_e) gets it at (q - c_e, e), and an open slot only gets
+// the force increment.
+__global__ void __launch_bounds__(128) k_fa_pull_fp64(const AaArgs a, const Trt<double> t) {
+  const int z = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * 4 + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= a.nZ || y >= a.nY) return;
+  const int c = aa_cell(a, x, y, z);
+  const uint32_t w = __ldg(a.link + c);
+  if (!(w & kFluidBit)) return;
+  const long long S = a.dstride;
+  const double* const f = a.f;
+  double* const g = launder(a.g);
+  auto load = [&](int d) -> double { return f[d * S + c - aa_off(a, d)]; };
+  auto store = [&](int e, double v) {
+    g[e * S + c] = v + t.force[e];
+    if (e == DC) return;
+    const int j = inv(e);
+    if (!((w >> e) & 1u)) {
+      const int q = aa_wrapped(a, x, y, z, e);
+      const int n = c + aa_off(a, e);
+      if (q != n) g[e * S + q - aa_off(a, e)] = v + t.force[e];  // periodic image's ghost slot
+    } else if (aa_open(a, x, y, z, e)) {
+      g[j * S + c + aa_off(a, e)] = g[j * S + c + aa_off(a, e)] + t.force[j];
+    } else {
+      g[j * S + c + aa_off(a, e)] = v + t.force[j];
+    }
+  };
+  trt_update(t, load, store);
+}
+
+void fa_push_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
+  k_fa_push_fp64<<<dim3((a.nZ + 31) / 32, (a.nY + 3) / 4, a.nX), dim3(32, 4), 0, s>>>(a, t);
+}
+void fa_pull_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
+  k_fa_pull_fp64<<<dim3((a.nZ + 31) / 32, (a.nY + 3) / 4, a.nX), dim3(32, 4), 0, s>>>(a, t);
+}
+
 long long aa_shell_cells(const AaArgs& a) {
   const long long sx = a.nX > 1 ? 2 : 1, sy = a.nY > 1 ? 2 : 1, sz = a.nZ > 1 ? 2 : 1;
   const long long mx = a.nX > 2 ? a.nX - 2 : 0, my = a.nY > 2 ? a.nY - 2 : 0;

@@ -320,6 +320,12 @@ static size_t aa_i(const orc_state_t *s, int x, int y, int z, int d)
  * Pull view: src/BenchKernelD3Q19ListPullSplitNtCommon.c:118-182. */
 static double *node_slot(orc_state_t *s, int x, int y, int z, int d)
 {
+	/* two-grid full array: push stores node x's PDFs at x, pull at x - c_d
+	 * (src/BenchKernelD3Q19Common.c:120-196) */
+	if (s->kind == ORC_KERNEL_PUSH_FA)
+		return &s->f[aa_i(s, x + 1, y + 1, z + 1, d)];
+	if (s->kind == ORC_KERNEL_PULL_FA)
+		return &s->f[aa_i(s, x + 1 - CX[d], y + 1 - CY[d], z + 1 - CZ[d], d)];
 	if (s->kind == ORC_KERNEL_AA) {
 		if (s->iteration % 2 == 0)
 			return &s->f[aa_i(s, x + 1 - CX[d], y + 1 - CY[d], z + 1 - CZ[d], INV[d])];
@@ -410,6 +416,47 @@ static void init_verify(orc_state_t *s, const int *lat, double omega, double rho
 /* AA full array: ghost-padded (n+2)^3 SoA, z fastest; fix-up lists for
  * periodic and bounce-back PDFs (src/BenchKernelD3Q19AaCommon.c:446-621). */
 
+/* Fix-up lists of the two-grid full-array pull kernel
+ * (src/BenchKernelD3Q19Common.c:531-660, PROP_MODEL_PULL): the neighbour a
+ * node pulls from is x - c_d; a wall or a wall behind a periodic wrap gets
+ * the node's own inverse PDF, a periodic ghost the image's PDF. */
+static void fa_build_pull_fixup(orc_state_t *s, const int *lat, const int periodic[3])
+{
+	int lx = s->nx, ly = s->ny, lz = s->nz;
+	int cap = 0;
+	for (size_t i = 0; i < (size_t)lx * ly * lz; ++i) if (lat[i] != 0) cap += Q;
+	s->bbSrc = (int *)malloc(sizeof(int) * (size_t)(cap + 1));
+	s->bbDst = (int *)malloc(sizeof(int) * (size_t)(cap + 1));
+	int k = 0;
+	for (int x = 0; x < lx; ++x) for (int y = 0; y < ly; ++y) for (int z = 0; z < lz; ++z) {
+		if (lat[LIDX(lx, ly, x, y, z)] == 0) continue;
+		for (int d = 0; d < Q; ++d) {
+			int nx = x - CX[d], ny = y - CY[d], nz = z - CZ[d];
+			int ox = nx < 0 || nx >= lx, oy = ny < 0 || ny >= ly, oz = nz < 0 || nz >= lz;
+			if ((ox && periodic[0]) || (oy && periodic[1]) || (oz && periodic[2])) {
+				int px = nx < 0 ? lx - 1 : (nx >= lx ? 0 : nx);
+				int py = ny < 0 ? ly - 1 : (ny >= ly ? 0 : ny);
+				int pz = nz < 0 ? lz - 1 : (nz >= lz ? 0 : nz);
+				if (lat[LIDX(lx, ly, px, py, pz)] == 0)
+					s->bbSrc[k] = (int)aa_i(s, x + 1, y + 1, z + 1, INV[d]);
+				else
+					s->bbSrc[k] = (int)aa_i(s, px + 1, py + 1, pz + 1, d);
+				s->bbDst[k] = (int)aa_i(s, nx + 1, ny + 1, nz + 1, d);
+				++k;
+			}
+			else if (ox || oy || oz) {
+				continue;
+			}
+			else if (lat[LIDX(lx, ly, nx, ny, nz)] == 0) {
+				s->bbSrc[k] = (int)aa_i(s, x + 1, y + 1, z + 1, INV[d]);
+				s->bbDst[k] = (int)aa_i(s, nx + 1, ny + 1, nz + 1, d);
+				++k;
+			}
+		}
+	}
+	s->nBB = k;
+}
+
 static void aa_build_fixup(orc_state_t *s, const int *lat, const int periodic[3])
 {
 	int lx = s->nx, ly = s->ny, lz = s->nz;
@@ -474,6 +521,29 @@ static void aa_odd(orc_state_t *s, const trt_t *t)
 			for (int d = 0; d < Q; ++d) s->f[aa_i(s, gx + CX[d], gy + CY[d], gz + CZ[d], d)] = o[d];
 		}
 	}
+}
+
+/* Two-grid full array (src/BenchKernelD3Q19.c:114-334): every interior cell,
+ * obstacles included, from grid f into grid g -- push: own PDFs in, PDF d out
+ * to x + c_d; pull: PDF d in from x - c_d, own PDFs out. The fix-up lists
+ * then run on g. */
+static void fa_step(orc_state_t *s, const trt_t *t, int pull)
+{
+	#pragma omp parallel for collapse(2)
+	for (int x = 0; x < s->nx; ++x) for (int y = 0; y < s->ny; ++y) {
+		for (int z = 0; z < s->nz; ++z) {
+			int gx = x + 1, gy = y + 1, gz = z + 1;
+			double f[Q], o[Q];
+			for (int d = 0; d < Q; ++d)
+				f[d] = pull ? s->f[aa_i(s, gx - CX[d], gy - CY[d], gz - CZ[d], d)] : s->f[aa_i(s, gx, gy, gz, d)];
+			trt_collide(t, f, o);
+			for (int d = 0; d < Q; ++d) {
+				if (pull) s->g[aa_i(s, gx, gy, gz, d)] = o[d];
+				else s->g[aa_i(s, gx + CX[d], gy + CY[d], gz + CZ[d], d)] = o[d];
+			}
+		}
+	}
+	for (int i = 0; i < s->nBB; ++i) s->g[s->bbDst[i]] = s->g[s->bbSrc[i]];
 }
 
 /* ------------------------------------------------------------------------ */
@@ -553,10 +623,15 @@ int orc_run(int kernel, const int dims[3], const int periodic[3], const int *lat
 	s.iteration = -1;
 	size_t ncell = (size_t)s.nx * s.ny * s.nz;
 
-	if (kernel == ORC_KERNEL_AA) {
+	const int fa = kernel == ORC_KERNEL_PUSH_FA || kernel == ORC_KERNEL_PULL_FA;
+	if (kernel == ORC_KERNEL_AA || fa) {
 		s.gx = s.nx + 2; s.gy = s.ny + 2; s.gz = s.nz + 2;
 		s.f = (double *)calloc((size_t)Q * s.gx * s.gy * s.gz, sizeof(double));
-		aa_build_fixup(&s, lattice, periodic);
+		if (kernel == ORC_KERNEL_PULL_FA)
+			fa_build_pull_fixup(&s, lattice, periodic);
+		else
+			aa_build_fixup(&s, lattice, periodic); /* the push lists of the two-grid kernel are the same */
+		if (fa) s.g = (double *)calloc((size_t)Q * s.gx * s.gy * s.gz, sizeof(double));
 	} else {
 		const int pull = kernel == ORC_KERNEL_LIST_PULL ? 1 : (kernel == ORC_KERNEL_LIST_PULL2 ? 2 : 0);
 		if (list_build(&s.L, pull, dims, periodic, lattice, blk, pad_mode, 0, NULL, NULL))
@@ -601,7 +676,9 @@ int orc_run(int kernel, const int dims[3], const int periodic[3], const int *lat
 		}
 	} else {
 		for (int it = 0; it < iterations; ++it) {
-			if (kernel == ORC_KERNEL_LIST_PUSH2)
+			if (fa)
+				fa_step(&s, &t, kernel == ORC_KERNEL_PULL_FA);
+			else if (kernel == ORC_KERNEL_LIST_PUSH2)
 				list_push2(&s, &t);
 			else
 				list_pull(&s, &t);
@@ -620,7 +697,7 @@ int orc_run(int kernel, const int dims[3], const int periodic[3], const int *lat
 	(void)ncell;
 
 	free(s.f); free(s.g); free(s.bbSrc); free(s.bbDst);
-	if (kernel != ORC_KERNEL_AA) list_free(&s.L);
+	if (kernel != ORC_KERNEL_AA && !fa) list_free(&s.L);
 	return 0;
 }
 

@@ -33,8 +33,11 @@ enum { ORC_GEO_BOX = 0, ORC_GEO_CHANNEL = 1, ORC_GEO_PIPE = 2, ORC_GEO_BLOCKS = 
  * LIST_PULL2 are the two-grid list kernels list-push-soa / list-pull-soa
  * (src/BenchKernelD3Q19List.c, layout src/BenchKernelD3Q19ListCommon.c:330-600,
  * padding only). */
+/* PUSH_FA / PULL_FA: the two-grid full-array kernels push-soa / pull-soa
+ * (src/BenchKernelD3Q19.c, layout and fix-up lists
+ * src/BenchKernelD3Q19Common.c:291-670). */
 enum { ORC_KERNEL_AA = 0, ORC_KERNEL_LIST_AA = 1, ORC_KERNEL_LIST_PULL = 2, ORC_KERNEL_LIST_PUSH2 = 3,
-       ORC_KERNEL_LIST_PULL2 = 4 };
+       ORC_KERNEL_LIST_PULL2 = 4, ORC_KERNEL_PUSH_FA = 5, ORC_KERNEL_PULL_FA = 6 };
 
 /* init modes */
 enum { ORC_INIT_ZERO = 0, ORC_INIT_VERIFY = 1, ORC_INIT_PDFS = 2 };

@@ -26,7 +26,7 @@ BUILD = os.path.join(HERE, "_build")
 REF = os.path.join(HERE, "_ref")
 
 GEO = {"box": 0, "channel": 1, "pipe": 2, "blocks": 3, "fluid": 4}
-KERNEL = {"aa": 0, "list-aa": 1, "list-pull": 2, "list-push2": 3, "list-pull2": 4}
+KERNEL = {"aa": 0, "list-aa": 1, "list-pull": 2, "list-push2": 3, "list-pull2": 4, "push-fa": 5, "pull-fa": 6}
 
 _i3 = ctypes.c_int * 3
 

@@ -23,11 +23,14 @@ KERNELS = [("cuda-aa-soa", "aa", "aa-soa"),
            ("cuda-list-aa-soa", "list-aa", "list-aa-soa"),
            ("cuda-list-aa-ria-soa", "list-aa", "list-aa-ria-soa"),
            ("cuda-list-push-soa", "list-push2", "list-push-soa"),
-           ("cuda-list-pull-soa", "list-pull2", "list-pull-soa")]
+           ("cuda-list-pull-soa", "list-pull2", "list-pull-soa"),
+           ("cuda-push-soa", "push-fa", "push-soa"),
+           ("cuda-pull-soa", "pull-fa", "pull-soa")]
 
 # reference kernels whose arithmetic is the scalar order (bit-identical to the
 # oracle); the others sum in SIMD order
-SCALAR_REFERENCE = {"aa-soa", "list-aa-soa", "list-aa-ria-soa", "list-push-soa", "list-pull-soa"}
+SCALAR_REFERENCE = {"aa-soa", "list-aa-soa", "list-aa-ria-soa", "list-push-soa", "list-pull-soa", "push-soa",
+                    "pull-soa"}
 
 EDGE_CASES = [
     ("fluid", (3, 3, 3), (1, 1, 1)),

@@ -40,7 +40,7 @@ def test_kernel_table_names():
     assert lbmb200.kernel_names() == ["cuda-aa-soa", "cuda-list-aa-pv-soa",
                                       "cuda-list-pull-split-nt-1s-soa", "cuda-list-pull-split-nt-2s-soa",
                                       "cuda-list-aa-soa", "cuda-list-aa-ria-soa", "cuda-list-push-soa",
-                                      "cuda-list-pull-soa"]
+                                      "cuda-list-pull-soa", "cuda-push-soa", "cuda-pull-soa"]
     # case-insensitive lookup as src/Main.c:543
     assert lbmb200.kernel("CUDA-AA-SOA").name == "cuda-aa-soa"
     with pytest.raises(KeyError):

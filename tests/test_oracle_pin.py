@@ -125,6 +125,8 @@ def test_other_list_layouts_match_reference(oracle, reference, kernel, pull, geo
     ("list-aa-ria-soa", "list-aa", True),
     ("list-push-soa", "list-push2", True),
     ("list-pull-soa", "list-pull2", True),
+    ("push-soa", "push-fa", True),
+    ("pull-soa", "pull-fa", True),
 ])
 @pytest.mark.parametrize("geo,dims,per", FIELD_CASES)
 def test_fields_match_reference(oracle, reference, kernel, okernel, exact, geo, dims, per):
@@ -142,7 +144,7 @@ def test_fields_match_reference(oracle, reference, kernel, okernel, exact, geo, 
         assert np.max(np.abs(r[m] - o[m]) / np.abs(r[m])) < 1e-13
 
 
-@pytest.mark.parametrize("okernel", ["aa", "list-aa", "list-pull", "list-push2", "list-pull2"])
+@pytest.mark.parametrize("okernel", ["aa", "list-aa", "list-pull", "list-push2", "list-pull2", "push-fa", "pull-fa"])
 def test_verify_known_answer_lambda_1_12(oracle, okernel):
     # reference -verify (16^3 box, periodic x/y, 1000 steps): 4.561374e-02
     dims, per = (16, 16, 16), (1, 1, 0)
@@ -151,7 +153,7 @@ def test_verify_known_answer_lambda_1_12(oracle, okernel):
     assert "%e" % oracle.verify_error(dims, lat, f) == "4.561374e-02"
 
 
-@pytest.mark.parametrize("okernel", ["aa", "list-aa", "list-pull", "list-push2", "list-pull2"])
+@pytest.mark.parametrize("okernel", ["aa", "list-aa", "list-pull", "list-push2", "list-pull2", "push-fa", "pull-fa"])
 def test_verify_known_answer_lambda_3_16(oracle, okernel):
     # reference with Lambda = 3/16 at the -verify preset: 7.855978e-02
     dims, per = (16, 16, 16), (1, 1, 0)
