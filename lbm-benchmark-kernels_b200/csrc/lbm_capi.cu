@@ -891,8 +891,13 @@ KernelData* lbm_aa_slab_init(LatticeDesc* global, int x0, int x1, int haloLo, in
     g_lastError = "slab range outside the lattice";
     return nullptr;
   }
-  if ((haloLo || haloHi) && global->PeriodicX == 0 && ((haloLo && x0 == 0) || (haloHi && x1 == nx))) {
-    g_lastError = "a halo face on the lattice's x boundary needs a periodic x axis";
+  // halo faces on the lattice's own x boundary close a ring: with periodic x,
+  // and also when only y or z is periodic, because a link that leaves through
+  // the x boundary and a periodic y/z face at once wraps every crossed axis
+  // (src/BenchKernelD3Q19AaCommon.c:522-578) and reaches the other x end
+  const bool anyPeriodic = global->PeriodicX || global->PeriodicY || global->PeriodicZ;
+  if (!anyPeriodic && ((haloLo && x0 == 0) || (haloHi && x1 == nx))) {
+    g_lastError = "a halo face on the lattice's x boundary needs a periodic axis";
     return nullptr;
   }
   const int L = x1 - x0;

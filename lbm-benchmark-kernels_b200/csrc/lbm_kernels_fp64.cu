@@ -236,19 +236,42 @@ __device__ __forceinline__ int halo_dir(int k, bool plusX) {
 }
 
 // plane: local x of the plane (-1 and nX are the ghost planes); plusX: which
-// five directions; toBuf: copy the slots into buf, else out of it.
-__global__ void k_aa_halo(const AaArgs a, int plane, bool plusX, bool toBuf, double* buf) {
+// five directions; mode: 0 copy the slots into buf; 1 (phase-0 unpack into a
+// ghost plane) and 2 (phase-1 unpack into a face plane) copy out of buf, but
+// only into the slots the odd step exchanges through the face:
+//  1: a ghost slot (g, y, z, d) is read and written by the face cell whose
+//     direct link d lands on it, (y - c_dy, z - c_dz) wrapped on the face;
+//     other ghost slots keep what they hold (open-face values);
+//  2: a face slot (y, z, d) was written by the neighbour only if this slab's
+//     cell reaches the neighbour's cell through the direct link inv(d); where
+//     that link is reversed (a wall or an open face behind the halo face),
+//     this slab's own odd step wrote the slot (bounce back) and keeps it.
+__global__ void k_aa_halo(const AaArgs a, int plane, bool plusX, int mode, double* buf) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long face = (long long)a.nY * a.nZ;
   if (i >= 5 * face) return;
   const int k = (int)(i / face);
   const int y = (int)(i % face / a.nZ), z = (int)(i % a.nZ);
-  const long long slot = halo_dir(k, plusX) * a.dstride + (long long)(plane + 1) * a.xs +
-                         (long long)(y + 1) * a.pitch + z + kZOff;
-  if (toBuf)
+  const int d = halo_dir(k, plusX);
+  const long long cell = (long long)(plane + 1) * a.xs + (long long)(y + 1) * a.pitch + z + kZOff;
+  const long long slot = d * a.dstride + cell;
+  if (mode == 0) {
     buf[i] = a.f[slot];
-  else
-    a.f[slot] = buf[i];
+    return;
+  }
+  bool take;
+  if (mode == 1) {
+    const int rx = plane < 0 ? 0 : a.nX - 1;
+    int ry = (y - cy(d)) % a.nY, rz = (z - cz(d)) % a.nZ;
+    ry += ry < 0 ? a.nY : 0;
+    rz += rz < 0 ? a.nZ : 0;
+    const uint32_t w = a.link[(long long)(rx + 1) * a.xs + (long long)(ry + 1) * a.pitch + rz + kZOff];
+    take = (w & kFluidBit) && !((w >> d) & 1u);
+  } else {
+    const uint32_t w = a.link[cell];
+    take = (w & kFluidBit) && !((w >> inv(d)) & 1u);
+  }
+  if (take) a.f[slot] = buf[i];
 }
 
 // Side 1 (x = nX-1 face): the cells of this slab cross it with c_x = +1, the
@@ -259,7 +282,7 @@ void aa_halo_pack(const AaArgs& a, int side, int phase, double* buf, cudaStream_
   // phase 0: the face plane's slots the neighbour streams through (pointing
   // into this slab); phase 1: the ghost plane's slots this slab streamed into
   const bool plusX = phase == 0 ? side == 0 : side == 1;
-  if (n > 0) k_aa_halo<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, plane, plusX, true, buf);
+  if (n > 0) k_aa_halo<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, plane, plusX, 0, buf);
 }
 
 void aa_halo_unpack(const AaArgs& a, int side, int phase, const double* buf, cudaStream_t s) {
@@ -267,7 +290,8 @@ void aa_halo_unpack(const AaArgs& a, int side, int phase, const double* buf, cud
   const int plane = phase == 0 ? (side == 0 ? -1 : a.nX) : (side == 0 ? 0 : a.nX - 1);
   const bool plusX = phase == 0 ? side == 1 : side == 0;
   if (n > 0)
-    k_aa_halo<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, plane, plusX, false, const_cast<double*>(buf));
+    k_aa_halo<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, plane, plusX, phase == 0 ? 1 : 2,
+                                                           const_cast<double*>(buf));
 }
 
 // ---------------------------------------------------------------------------

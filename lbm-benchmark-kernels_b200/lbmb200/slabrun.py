@@ -37,12 +37,17 @@ def main(argv=None):
         per = tuple(int(c in a.periodic) for c in "xyz")
         lat = lbmb200.geometry(a.geometry, dims, per)
         x0, x1 = sl.partition(dims[0], ranks.world)[ranks.rank]
-        lo, hi = sl.halo_flags(ranks.rank, ranks.world, lat.periodic[0])
+        ring = sl.is_ring(lat.periodic)
+        lo, hi = sl.halo_flags(ranks.rank, ranks.world, ring)
         lbmb200.lib().lbm_b200_set_device(ranks.local)
         torch.cuda.set_device(ranks.local)
         slab = sl.Slab(lat, x0, x1, lo, hi, kernel_args=["-lambda", a.lam])
-        stream = torch.cuda.current_stream().cuda_stream
-        tr = sl.DistTransport(slab, ranks.rank, ranks.world, lat.periodic[0], dist,
+        # an explicit stream, current for torch.distributed too: kernels,
+        # packs, the library's sends/receives and unpacks run in one order
+        work = torch.cuda.Stream()
+        torch.cuda.set_stream(work)
+        stream = work.cuda_stream
+        tr = sl.DistTransport(slab, ranks.rank, ranks.world, ring, dist,
                               lambda n: torch.empty(n, dtype=torch.float64, device="cuda"), stream=stream)
         cd = lbmb200.case(omega=a.omega, xforce=1e-5)
         sl.step_pairs([slab], tr, cd, a.warmup, stream)

@@ -22,6 +22,8 @@ Transports: ``LocalTransport`` (all slabs in this process: device-to-device
 through shared device buffers, every operation on one stream) and
 ``DistTransport`` (one slab per rank: paired isend/irecv through
 torch.distributed -- NCCL on GPUs, gloo on CPU for the host-side tests).
+The slabs close into a ring (the first and last slab exchange too) when any
+axis is periodic (``is_ring``).
 """
 import ctypes
 
@@ -38,16 +40,24 @@ def partition(nx, parts):
     return list(zip(edges[:-1], edges[1:]))
 
 
-def halo_flags(rank, parts, periodic_x):
+def is_ring(periodic):
+    """Whether the slabs close into a ring: with a periodic x axis, and also
+    with only y or z periodic, since a link that leaves through the x boundary
+    and a periodic face at once wraps every crossed axis to the other x end
+    (the reference's rule, src/BenchKernelD3Q19AaCommon.c:522-578)."""
+    return any(bool(p) for p in periodic)
+
+
+def halo_flags(rank, parts, ring):
     """(halo at the x0 face, halo at the x1-1 face) of slab `rank`."""
     if parts == 1:
         return False, False
-    return (rank > 0 or bool(periodic_x)), (rank < parts - 1 or bool(periodic_x))
+    return (rank > 0 or bool(ring)), (rank < parts - 1 or bool(ring))
 
 
-def neighbours(rank, parts, periodic_x):
+def neighbours(rank, parts, ring):
     """(left, right) neighbour slab of `rank` (None at a closed x face)."""
-    lo, hi = halo_flags(rank, parts, periodic_x)
+    lo, hi = halo_flags(rank, parts, ring)
     return ((rank - 1) % parts if lo else None), ((rank + 1) % parts if hi else None)
 
 
@@ -117,13 +127,17 @@ class Slab:
 class LocalTransport:
     """All slabs of the lattice in this process, on one device: messages go
     through device buffers, and every step, pack and unpack is enqueued on
-    one stream, so they run in program order."""
+    one stream, so they run in program order. The stream must be an explicit
+    one: the library puts operations given a null stream on each instance's
+    own stream, which would not order the slabs' operations."""
 
-    def __init__(self, slabs, periodic_x, stream, alloc):
+    def __init__(self, slabs, ring, stream, alloc):
+        if not stream:
+            raise ValueError("LocalTransport needs an explicit (non-null) stream")
         self.slabs, self.stream = slabs, stream
         n = len(slabs)
         # faces between slab r (side 1) and its right-hand neighbour (side 0)
-        self.faces = [(r, (r + 1) % n) for r in range(n) if neighbours(r, n, periodic_x)[1] is not None]
+        self.faces = [(r, (r + 1) % n) for r in range(n) if neighbours(r, n, ring)[1] is not None]
         self.bufs = {f: (alloc(slabs[f[0]].count), alloc(slabs[f[0]].count)) for f in self.faces}
 
     def exchange(self, phase):
@@ -141,9 +155,9 @@ class DistTransport:
     receives left face first, so that two messages between the same pair of
     ranks (two slabs on a periodic ring) match in order."""
 
-    def __init__(self, slab, rank, world, periodic_x, dist, make_buf, stream=None):
+    def __init__(self, slab, rank, world, ring, dist, make_buf, stream=None):
         self.slab, self.dist, self.stream = slab, dist, stream
-        self.left, self.right = neighbours(rank, world, periodic_x)
+        self.left, self.right = neighbours(rank, world, ring)
         self.send = {s: make_buf(slab.count) for s in (0, 1)}
         self.recv = {s: make_buf(slab.count) for s in (0, 1)}
 

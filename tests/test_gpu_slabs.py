@@ -14,6 +14,9 @@ pytestmark = pytest.mark.gpu
 
 CASES = [
     ("fluid", (24, 10, 12), (1, 1, 1), 2),
+    ("box", (12, 9, 8), (0, 1, 1), 3),       # x closed, y/z periodic: edge links wrap to the other x end
+    ("fluid", (5, 6, 7), (0, 1, 1), 5),
+    ("fluid", (9, 8, 7), (0, 1, 0), 3),
     ("fluid", (25, 9, 11), (1, 1, 1), 3),    # uneven slabs, periodic ring
     ("fluid", (9, 8, 7), (1, 0, 1), 4),      # thin slabs, corner links wrap on several axes
     ("fluid", (6, 7, 8), (1, 1, 0), 3),      # two-plane slabs, open z faces
@@ -26,13 +29,15 @@ CASES = [
 
 def _run_slabs(lat, parts, init, cd, pairs):
     import torch
-    stream = torch.cuda.current_stream().cuda_stream
+    work = torch.cuda.Stream()  # an explicit stream orders all slabs' operations
+    stream = work.cuda_stream
+    ring = sl.is_ring(lat.periodic)
     ranges = sl.partition(lat.dims[0], parts)
-    slabs = [sl.Slab(lat, x0, x1, *sl.halo_flags(r, parts, lat.periodic[0]), kernel_args=["-lambda", "3/16"])
+    slabs = [sl.Slab(lat, x0, x1, *sl.halo_flags(r, parts, ring), kernel_args=["-lambda", "3/16"])
              for r, (x0, x1) in enumerate(ranges)]
     try:
         sl.scatter_field(slabs, lat, init)
-        tr = sl.LocalTransport(slabs, lat.periodic[0], stream,
+        tr = sl.LocalTransport(slabs, ring, stream,
                                lambda n: torch.empty(n, dtype=torch.float64, device="cuda"))
         sl.step_pairs(slabs, tr, cd, pairs, stream)
         torch.cuda.synchronize()
@@ -60,7 +65,7 @@ def test_slabs_equal_whole_lattice(geo, dims, per, parts):
 
 
 def test_slab_refuses_halo_on_closed_boundary():
-    lat = lbmb200.geometry("channel", (12, 8, 8), (0, 0, 0))
+    lat = lbmb200.geometry("fluid", (12, 8, 8), (0, 0, 0))
     with pytest.raises(RuntimeError, match="periodic"):
         sl.Slab(lat, 0, 6, True, True)
 

@@ -34,7 +34,7 @@ SCRIPT = textwrap.dedent("""
     r = Ranks(backend="gloo", timeout_s=30)
     periodic = int(sys.argv[1])
     slab = FakeSlab(r.rank)
-    tr = sl.DistTransport(slab, r.rank, r.world, periodic, dist,
+    tr = sl.DistTransport(slab, r.rank, r.world, sl.is_ring((periodic, 0, 0)), dist,
                           lambda n: torch.zeros(n, dtype=torch.float64))
     tr.exchange(0)
     tr.exchange(1)
