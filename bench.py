@@ -510,6 +510,16 @@ def run_ours(args, dist):
             extra[key] = aa_line(lbmb200, fl, args, kargs, dist, peak)
             extra[key]["workload"] = "%d^3 %s" % (args.edge, "fully periodic fluid box" if geo == "fluid"
                                                   else "channel, periodic x, walls in y and z")
+        # the two-grid full-array rows on the fluid box (304 B per node update)
+        fl = lbmb200.geometry("fluid", (args.edge,) * 3, (1, 1, 1))
+        for kname in ("cuda-push-soa", "cuda-pull-soa"):
+            tq = time_kernel(lbmb200, kname, fl, min(args.steps, 100), 3, kargs, dist, "aa")
+            tq["inst"].deinit()
+            qm = statistics.mean(tq["per_launch_ms"])
+            extra[kname] = {"workload": "%d^3 fully periodic fluid box" % args.edge,
+                            "mflups": round(fl.n_fluid / (qm / 1e3) / 1e6, 1), "launch_ms": round(qm, 5),
+                            "achieved_gbs": round(B_PER_FLUP["aa"] * fl.n_fluid / (qm / 1e3) / 1e9, 1),
+                            "frac": round(B_PER_FLUP["aa"] * fl.n_fluid / (qm / 1e3) / 1e9 / peak, 4)}
         # reduced storage list AA on the porous domain (FP32 arithmetic)
         for prec, pb in (("fp32", 4), ("fp16", 2)):
             tl = time_kernel(lbmb200, "cuda-list-aa-pv-soa", lat, min(args.steps, 200), 4,

@@ -575,6 +575,11 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* sla
     g->pitch = (ld->Dims[2] + lbm::kZOff + 1 + 3) / 4 * 4;
     g->xs = gy * g->pitch;
     g->dstride = (long long)gx * g->xs;
+    if (ld->Dims[0] > 65535 || ld->Dims[1] > 65535) {
+      // the full-array kernels put x and y on the grid's y/z dimensions
+      std::printf("ERROR: the full-array kernels take at most 65535 cells along x and y.\n");
+      std::exit(1);
+    }
     if ((unsigned long long)Q * g->dstride >= (1ull << 31)) {
       // the odd step addresses all 19 planes with 32-bit offsets (the
       // reference bounds its PDF count by 2^31 too, src/Main.c:399-406)

@@ -64,9 +64,12 @@ __device__ __forceinline__ bool aa_open(const AaArgs& a, int x, int y, int z, in
   return (ox || oy || oz) && !crossesPeriodic;
 }
 
-__global__ void __launch_bounds__(128) k_aa_even_fp64(const AaArgs a, const Trt<double> t) {
-  const int z = blockIdx.x * 32 + threadIdx.x;
-  const int y = blockIdx.y * 4 + threadIdx.y;
+// One block per 128 z-cells of a row (longer contiguous segments per plane
+// than 32 x 4 blocks), capped at 8 resident blocks per SM (64 registers):
+// 0.827 ms against 0.850 ms for 32 x 4 blocks at 256^3 on B200.
+__global__ void __launch_bounds__(128, 8) k_aa_even_fp64(const AaArgs a, const Trt<double> t) {
+  const int z = blockIdx.x * 128 + threadIdx.x;
+  const int y = blockIdx.y;
   const int x = blockIdx.z;
   if (z >= a.nZ || y >= a.nY) return;
   const int c = aa_cell(a, x, y, z);
@@ -422,10 +425,8 @@ void aa_interior_blocks(const AaArgs& a, const uint32_t* link, int* blocks, int*
   for (int id : general) blocks[*nDirect + (*nGeneral)++] = id;
 }
 
-static dim3 aa_grid(const AaArgs& a) { return dim3((a.nZ + 31) / 32, (a.nY + 3) / 4, a.nX); }
-
 void aa_even_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
-  k_aa_even_fp64<<<aa_grid(a), dim3(32, 4), 0, s>>>(a, t);
+  k_aa_even_fp64<<<dim3((a.nZ + 127) / 128, a.nY, a.nX), 128, 0, s>>>(a, t);
 }
 
 void aa_odd_interior_fp64(const AaArgs& a, const Trt<double>& t, const int* blocks, int nDirect, int nGeneral,

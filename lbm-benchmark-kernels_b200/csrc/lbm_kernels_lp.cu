@@ -2,6 +2,8 @@
 // in HBM as FP32 or FP16 deviations from the lattice weights (lbm_store.cuh),
 // with the collision evaluated in FP32 (FMA contraction allowed in this file).
 // Bytes per fluid-lattice update: even 19*2*s, odd 19*2*s + 72 (s = 4 or 2).
+#include <type_traits>
+
 #include "lbm_bulk.cuh"
 #include "lbm_kernels.cuh"
 #include "lbm_store.cuh"
@@ -69,14 +71,43 @@ __global__ void __launch_bounds__(256) k_list_even_staged(const ListArgsLp a, co
       return;
     }
     const T* buf = reinterpret_cast<const T*>(stage + (size_t)st * Q * StageBytes);
+    if constexpr (std::is_same<St, StoreF16>::value) {
+      // FP16: two neighbouring nodes per thread, moved as half2 (one shared
+      // memory load, one conversion and one 4-byte store per direction for
+      // both); a pair's second node past nFluid is a padding node, whose
+      // zero deviations relax to zero
 #pragma unroll 1
-    for (int k = 0; k < NPT; ++k) {
-      const int local = threadIdx.x + k * 256;
-      const int n = tile * TN + local;
-      if (n >= a.nFluid) break;
-      T* const fs = launder(f + n);
-      trt_update(t, [&](int d) { return St::dev(buf[d * TN + local], d); },
-                 [&](int d, float v) { fs[inv(d) * S] = St::raw(v, inv(d)); });
+      for (int k = 0; k < NPT / 2; ++k) {
+        const int local = 2 * (threadIdx.x + k * 256);
+        const int n = tile * TN + local;
+        if (n >= a.nFluid) break;
+        float fa[Q], fb[Q], oa[Q], ob[Q];
+#pragma unroll
+        for (int d = 0; d < Q; ++d) {
+          const float2 v = __half22float2(*reinterpret_cast<const __half2*>(buf + d * TN + local));
+          const float inv_s = 1.0f / StoreF16::scale(d);
+          fa[d] = v.x * inv_s;
+          fb[d] = v.y * inv_s;
+        }
+        trt_collide(t, fa, oa);
+        trt_collide(t, fb, ob);
+        T* const fs = launder(f + n);
+#pragma unroll
+        for (int d = 0; d < Q; ++d) {
+          const float sc = StoreF16::scale(inv(d));
+          *reinterpret_cast<__half2*>(fs + inv(d) * S) = __floats2half2_rn(oa[d] * sc, ob[d] * sc);
+        }
+      }
+    } else {
+#pragma unroll 1
+      for (int k = 0; k < NPT; ++k) {
+        const int local = threadIdx.x + k * 256;
+        const int n = tile * TN + local;
+        if (n >= a.nFluid) break;
+        T* const fs = launder(f + n);
+        trt_update(t, [&](int d) { return St::dev(buf[d * TN + local], d); },
+                   [&](int d, float v) { fs[inv(d) * S] = St::raw(v, inv(d)); });
+      }
     }
   }
 }
