@@ -252,30 +252,59 @@ int lbm_b200_time_steps(KernelData *kd, CaseData *cd, int n, double *total_ms, d
  * reversed links; face shell), list AA 2 per pair, pull 1 per step. */
 long lbm_b200_launches_for(KernelData *kd, int n);
 
-/* ---- x-slabs of a full-array AA lattice (one lattice over several GPUs) ----
+/* ---- x-slabs of an AA-pattern lattice (one lattice over several GPUs) ----
+ * No counterpart in the reference, whose kernels address one array; the
+ * slabs reproduce the undivided lattice's run bit for bit.
+ *
  * lbm_aa_slab_init: an AA instance (the cuda-aa-soa kernels, Parameters as
  * its Init) over the x range [x0, x1) of `global`, in local coordinates
  * (local x = x - x0; GetNode/SetNode/get_field use a LatticeDesc of the slab).
  * Link words come from the whole lattice, so a link into a neighbouring slab
  * is direct exactly when the global neighbour is fluid. haloLo / haloHi: the
  * x = x0 / x = x1-1 face borders a neighbour slab (on the lattice's own x
- * boundary only with periodic x: the ring's wrap). Returns NULL on errors
- * (lbm_b200_last_error).
+ * boundary only with a periodic axis: the ring's wrap). Returns NULL on
+ * errors (lbm_b200_last_error).
+ *
+ * lbm_aa_list_slab_init: the same for the list AA kernel
+ * (cuda-list-aa-pv-soa, FP64 storage): the slab's fluid cells are the owned
+ * nodes (the kernel's blocked numbering over the slab), followed by ghost
+ * nodes for the fluid cells of the neighbouring slabs that owned links reach;
+ * adjacency follows the whole lattice's link rule.
+ *
  * A step pair is: lbm_aa_slab_step(half 0, even step) on every slab; for
  * every halo face, lbm_aa_halo_pack(side, 0) -> send to the neighbour ->
  * lbm_aa_halo_unpack(side, 0) there; lbm_aa_slab_step(half 1, odd step); the
- * same exchange with phase 1. side 0 is the x0 face, 1 the x1-1 face; a
- * message is lbm_aa_halo_count doubles (5 directions x nY x nZ) in device
- * memory. Pack of (side 1, phase p) pairs with unpack of (side 0, phase p) on
- * the right-hand neighbour and vice versa. The functions enqueue on `stream`
- * (NULL: the instance's stream) and return 0 or an error code; after steps on
- * another stream, synchronise it before lbm_b200_sync_mirror. */
+ * same exchange with phase 1. side 0 is the x0 face, 1 the x1-1 face.
+ * Pack of (side 1, phase p) pairs with unpack of (side 0, phase p) on the
+ * right-hand neighbour and vice versa. Messages are doubles in device
+ * memory: lbm_aa_halo_message(side, phase, send) of them go out (send = 1)
+ * or come in (send = 0) through a face -- 5 x nY x nZ for full-array slabs,
+ * the face's link count for list slabs (-1: no halo on that face);
+ * lbm_aa_halo_count is the largest message of the slab. The functions
+ * enqueue on `stream` (NULL: the instance's stream) and return 0 or an error
+ * code; after steps on another stream, synchronise it before
+ * lbm_b200_sync_mirror. */
 KernelData *lbm_aa_slab_init(LatticeDesc *global, int x0, int x1, int haloLo, int haloHi, Parameters *params);
+KernelData *lbm_aa_list_slab_init(LatticeDesc *global, int x0, int x1, int haloLo, int haloHi, Parameters *params);
 void lbm_aa_slab_deinit(KernelData *kd);
 long long lbm_aa_halo_count(KernelData *kd);
+long long lbm_aa_halo_message(KernelData *kd, int side, int phase, int send);
 int lbm_aa_halo_pack(KernelData *kd, int side, int phase, double *buf, void *stream);
 int lbm_aa_halo_unpack(KernelData *kd, int side, int phase, const double *buf, void *stream);
 int lbm_aa_slab_step(KernelData *kd, CaseData *cd, int half, void *stream);
+
+/* The layout lbm_aa_list_slab_init builds, on the host only (no CUDA call):
+ * counts[0..6] = owned nodes, ghost nodes, nCells, then the lengths of the
+ * own / ghost slot lists of side 0 and of side 1 (-1: no halo). Non-NULL
+ * arrays receive the slab's numbering (x1-x0 by nY by nZ cells, x fastest;
+ * obstacles 0xffffffff), the adjacency (owned nodes x 18, indices into
+ * f[d * nCells + node]) and the four slot lists: own = the owned slots the
+ * neighbour's face cells reach through that face (sent in phase 0, received
+ * in phase 1), ghost = the ghost slots this slab's face cells reach
+ * (received in phase 0, sent in phase 1). Returns 0 or a negative error. */
+int lbm_aa_list_slab_layout(const LatticeDesc *global, int x0, int x1, int haloLo, int haloHi, Parameters *params,
+                            long long *counts, uint32_t *grid, uint32_t *adj, uint32_t *ownLo, uint32_t *ghostLo,
+                            uint32_t *ownHi, uint32_t *ghostHi);
 
 /* Runs a kernel that waits, with a bound of `polls` reads, on a device flag
  * that nothing sets: the wait runs out, the kernel records error bit 2 in its

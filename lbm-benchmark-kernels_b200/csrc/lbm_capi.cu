@@ -11,6 +11,7 @@
 // GetNode/SetNode; Kernel uploads it when SetNode has touched it, runs the time
 // steps back to back on the instance's stream, and downloads it afterwards.
 #include <algorithm>
+#include <atomic>
 #include <cerrno>
 #include <chrono>
 #include <cstdio>
@@ -73,6 +74,11 @@ struct Gpu {
   // x-slab of a larger lattice (lbm_aa_slab_init): halo/cross flags of the two x faces
   int halo[2], cross[2];
   int* sliceMask;          // the slab's own mask (owned)
+  // x-slab of a list-AA lattice (lbm_aa_list_slab_init): halo slot lists per
+  // side, [side][0] = own slots the neighbour reaches, [side][1] = ghost slots
+  uint32_t* dHalo[2][2];
+  long long nHalo[2][2];
+  bool listSlab;
 
   // list layout
   uint32_t* grid;
@@ -288,8 +294,22 @@ lbm::AaArgs aa_args(Gpu* g) {
   return a;
 }
 
+// Whether list steps prefetch the adjacency of later tiles into L2
+// (LBM_ADJ_PREFETCH=0 turns it off; the launchers pick the distance).
+int list_prefetch_enabled() {
+  static std::atomic<int> on{-1};
+  int v = on.load(std::memory_order_acquire);
+  if (v < 0) {
+    const char* env = std::getenv("LBM_ADJ_PREFETCH");
+    v = (env && *env && std::atoi(env) == 0) ? 0 : 1;
+    on.store(v, std::memory_order_release);
+  }
+  return v;
+}
+
 lbm::ListArgs list_args(Gpu* g) {
   lbm::ListArgs a;
+  a.prefetch = list_prefetch_enabled();
   a.f = g->cur == 0 ? g->dF : g->dG;
   a.g = g->cur == 0 ? g->dG : g->dF;
   a.adj = g->dAdj;
@@ -301,6 +321,7 @@ lbm::ListArgs list_args(Gpu* g) {
 
 lbm::ListArgsLp list_args_lp(Gpu* g) {
   lbm::ListArgsLp a;
+  a.prefetch = list_prefetch_enabled();
   a.f = g->dF;
   a.adj = g->dAdj;
   a.nCells = g->nCells;
@@ -529,6 +550,7 @@ struct SlabSpec {
   const LatticeDesc* global;
   int x0, x1;
   int halo[2];
+  LbmhListSlab* list;  // list layout of a list-AA slab (ownership moves to the instance)
 };
 
 Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* slab = nullptr) {
@@ -646,6 +668,27 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* sla
     // keeps the numbering for GetNode/SetNode
     LBM_CK(cudaMalloc(&g->dAdj, sizeof(uint32_t) * adjElems));
     LBM_CK(cudaMemset(g->dAdj, 0, sizeof(uint32_t) * adjElems));
+    if (slab && slab->list) {
+      // a list-AA slab: the host-built layout with ghost nodes after the owned ones
+      LbmhListSlab* ls = slab->list;
+      g->nCells = nCells = ls->nCells;
+      std::free(g->grid);
+      g->grid = ls->grid;
+      ls->grid = nullptr;
+      if (ls->nOwned > 0)
+        LBM_CK(cudaMemcpy(g->dAdj, ls->adj, sizeof(uint32_t) * QM * (size_t)ls->nOwned, cudaMemcpyHostToDevice));
+      for (int side = 0; side < 2; ++side)
+        for (int list = 0; list < 2; ++list) {
+          const uint32_t* h = list == 0 ? ls->own[side] : ls->ghost[side];
+          const long n = list == 0 ? ls->nOwnSlots[side] : ls->nGhostSlots[side];
+          g->nHalo[side][list] = h ? n : -1;
+          if (h && n > 0) {
+            LBM_CK(cudaMalloc(&g->dHalo[side][list], sizeof(uint32_t) * (size_t)n));
+            LBM_CK(cudaMemcpy(g->dHalo[side][list], h, sizeof(uint32_t) * (size_t)n, cudaMemcpyHostToDevice));
+          }
+        }
+      g->listSlab = true;
+    }
     int* dMask = nullptr;
     uint32_t* dGrid = nullptr;
     LBM_CK(cudaMalloc(&dMask, sizeof(int) * ncell));
@@ -653,13 +696,15 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* sla
     LBM_CK(cudaMemcpy(dMask, ld->Lattice, sizeof(int) * ncell, cudaMemcpyHostToDevice));
     const int per3[3] = {ld->PeriodicX, ld->PeriodicY, ld->PeriodicZ};
     const char* berr = "";
-    const long long nf = lbm::list_build_device(dMask, ld->Dims, per3, pull ? 1 : 0, a.blk, nCells, dGrid, g->dAdj,
-                                                nTiles * lbm::kListTile, g->stream, &berr);
-    if (nf != g->nFluid) {
-      std::printf("ERROR: list build: %s (fluid nodes %lld, expected %d).\n", berr, nf, g->nFluid);
-      std::exit(1);
+    if (!g->listSlab) {
+      const long long nf = lbm::list_build_device(dMask, ld->Dims, per3, pull ? 1 : 0, a.blk, nCells, dGrid, g->dAdj,
+                                                  nTiles * lbm::kListTile, g->stream, &berr);
+      if (nf != g->nFluid) {
+        std::printf("ERROR: list build: %s (fluid nodes %lld, expected %d).\n", berr, nf, g->nFluid);
+        std::exit(1);
+      }
+      LBM_CK(cudaMemcpy(g->grid, dGrid, sizeof(uint32_t) * ncell, cudaMemcpyDeviceToHost));
     }
-    LBM_CK(cudaMemcpy(g->grid, dGrid, sizeof(uint32_t) * ncell, cudaMemcpyDeviceToHost));
     LBM_CK(cudaFree(dGrid));
     LBM_CK(cudaFree(dMask));
     g->mirrorElems = (size_t)Q * nCells;
@@ -702,6 +747,8 @@ void gpu_free(KernelData** kernelData) {
   cudaFree(g->dOddBlocks);
   std::free(g->sliceMask);
   cudaFree(g->dAdj);
+  for (int side = 0; side < 2; ++side)
+    for (int list = 0; list < 2; ++list) cudaFree(g->dHalo[side][list]);
   cudaFree(g->dErr);
   cudaFree(g->dMomOut);
   cudaFreeHost(g->mirror);
@@ -888,10 +935,34 @@ const char* lbm_b200_last_error(void) { return g_lastError.c_str(); }
 
 long lbm_b200_launches_for(KernelData* kd, int n) { return launches_for(reinterpret_cast<Gpu*>(kd), n); }
 
-// --- x-slabs of a full-array AA lattice ----------------------------------------
+// --- x-slabs of an AA-pattern lattice (full-array and list layouts) -------------
+
+// The slab's own cells of `global` as a lattice of its own (mask owned by the
+// caller): x range [x0, x1), the other axes whole.
+static int* slab_mask(const LatticeDesc* global, int x0, int x1, LatticeDesc* local) {
+  const int nx = global->Dims[0], ny = global->Dims[1], nz = global->Dims[2];
+  const int L = x1 - x0;
+  int* mask = static_cast<int*>(std::malloc(sizeof(int) * (size_t)L * ny * nz));
+  if (!mask) return nullptr;
+  int nFluid = 0;
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < L; ++x) {
+        const int v = global->Lattice[((long)z * ny + y) * nx + x0 + x];
+        mask[((long)z * ny + y) * L + x] = v;
+        nFluid += v != LAT_CELL_OBSTACLE;
+      }
+  *local = *global;
+  local->Dims[0] = L;
+  local->Lattice = mask;
+  local->nCells = L * ny * nz;
+  local->nFluid = nFluid;
+  local->nObst = local->nCells - nFluid;
+  return mask;
+}
 
 KernelData* lbm_aa_slab_init(LatticeDesc* global, int x0, int x1, int haloLo, int haloHi, Parameters* params) {
-  const int nx = global->Dims[0], ny = global->Dims[1], nz = global->Dims[2];
+  const int nx = global->Dims[0];
   if (x0 < 0 || x1 > nx || x1 - x0 < 1) {
     g_lastError = "slab range outside the lattice";
     return nullptr;
@@ -905,27 +976,80 @@ KernelData* lbm_aa_slab_init(LatticeDesc* global, int x0, int x1, int haloLo, in
     g_lastError = "a halo face on the lattice's x boundary needs a periodic axis";
     return nullptr;
   }
-  const int L = x1 - x0;
-  int* mask = static_cast<int*>(std::malloc(sizeof(int) * (size_t)L * ny * nz));
+  LatticeDesc local;
+  int* mask = slab_mask(global, x0, x1, &local);
   if (!mask) return nullptr;
-  int nFluid = 0;
-  for (int z = 0; z < nz; ++z)
-    for (int y = 0; y < ny; ++y)
-      for (int x = 0; x < L; ++x) {
-        const int v = global->Lattice[((long)z * ny + y) * nx + x0 + x];
-        mask[((long)z * ny + y) * L + x] = v;
-        nFluid += v != LAT_CELL_OBSTACLE;
-      }
-  LatticeDesc local = *global;
-  local.Dims[0] = L;
-  local.Lattice = mask;
-  local.nCells = L * ny * nz;
-  local.nFluid = nFluid;
-  local.nObst = local.nCells - nFluid;
-  SlabSpec spec{global, x0, x1, {haloLo != 0, haloHi != 0}};
+  SlabSpec spec{global, x0, x1, {haloLo != 0, haloHi != 0}, nullptr};
   Gpu* g = gpu_new(kAa, &local, params, &spec);
   g->sliceMask = mask;
   return &g->kd;
+}
+
+static const char* list_slab_error(int rc) {
+  switch (rc) {
+    case -1: return "slab range outside the lattice, or a halo on a slab that spans it";
+    case -2: return "a link leaves the slab through an x face without a halo";
+    case -3: return "allocation failed";
+    case -4: return "malformed -pad string";
+    case -5: return "the slab's PDFs exceed 32-bit indices";
+    default: return "list slab build failed";
+  }
+}
+
+KernelData* lbm_aa_list_slab_init(LatticeDesc* global, int x0, int x1, int haloLo, int haloHi, Parameters* params) {
+  const Args a = parse_args(params);
+  if (a.storage != lbm::kStoreF64) {
+    g_lastError = "list slabs store FP64 PDFs";
+    return nullptr;
+  }
+  LbmhListSlab ls;
+  const int halo[2] = {haloLo != 0, haloHi != 0};
+  const int rc = lbmh_list_slab_build(global, x0, x1, halo, a.blk, a.pad, &ls);
+  if (rc) {
+    g_lastError = list_slab_error(rc);
+    return nullptr;
+  }
+  LatticeDesc local;
+  int* mask = slab_mask(global, x0, x1, &local);
+  if (!mask) {
+    lbmh_list_slab_free(&ls);
+    g_lastError = "allocation failed";
+    return nullptr;
+  }
+  SlabSpec spec{global, x0, x1, {halo[0], halo[1]}, &ls};
+  Gpu* g = gpu_new(kListAa, &local, params, &spec);
+  g->sliceMask = mask;
+  lbmh_list_slab_free(&ls);
+  return &g->kd;
+}
+
+int lbm_aa_list_slab_layout(const LatticeDesc* global, int x0, int x1, int haloLo, int haloHi, Parameters* params,
+                            long long* counts, uint32_t* grid, uint32_t* adj, uint32_t* ownLo, uint32_t* ghostLo,
+                            uint32_t* ownHi, uint32_t* ghostHi) {
+  const Args a = parse_args(params);
+  LbmhListSlab ls;
+  const int halo[2] = {haloLo != 0, haloHi != 0};
+  const int rc = lbmh_list_slab_build(global, x0, x1, halo, a.blk, a.pad, &ls);
+  if (rc) {
+    g_lastError = list_slab_error(rc);
+    return rc;
+  }
+  counts[0] = ls.nOwned;
+  counts[1] = ls.nGhost;
+  counts[2] = ls.nCells;
+  counts[3] = ls.own[0] ? ls.nOwnSlots[0] : -1;
+  counts[4] = ls.ghost[0] ? ls.nGhostSlots[0] : -1;
+  counts[5] = ls.own[1] ? ls.nOwnSlots[1] : -1;
+  counts[6] = ls.ghost[1] ? ls.nGhostSlots[1] : -1;
+  const size_t cells = (size_t)ls.L * global->Dims[1] * global->Dims[2];
+  if (grid) std::memcpy(grid, ls.grid, sizeof(uint32_t) * cells);
+  if (adj && ls.nOwned > 0) std::memcpy(adj, ls.adj, sizeof(uint32_t) * QM * (size_t)ls.nOwned);
+  uint32_t* outs[4] = {ownLo, ghostLo, ownHi, ghostHi};
+  const uint32_t* ins[4] = {ls.own[0], ls.ghost[0], ls.own[1], ls.ghost[1]};
+  for (int k = 0; k < 4; ++k)
+    if (outs[k] && ins[k] && counts[3 + k] > 0) std::memcpy(outs[k], ins[k], sizeof(uint32_t) * (size_t)counts[3 + k]);
+  lbmh_list_slab_free(&ls);
+  return 0;
 }
 
 void lbm_aa_slab_deinit(KernelData* kd) {
@@ -933,9 +1057,22 @@ void lbm_aa_slab_deinit(KernelData* kd) {
   gpu_free(&k);
 }
 
+long long lbm_aa_halo_message(KernelData* kd, int side, int phase, int send) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (side < 0 || side > 1 || phase < 0 || phase > 1) return -1;
+  if (!g->listSlab) return g->kind == kAa ? 5LL * g->dims[1] * g->dims[2] : -1;
+  // phase 0 sends the own slots and receives the ghosts; phase 1 the reverse
+  const int list = (phase == 0) == (send != 0) ? 0 : 1;
+  return g->nHalo[side][list];
+}
+
 long long lbm_aa_halo_count(KernelData* kd) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
-  return 5LL * g->dims[1] * g->dims[2];
+  if (!g->listSlab) return 5LL * g->dims[1] * g->dims[2];
+  long long m = 0;
+  for (int side = 0; side < 2; ++side)
+    for (int list = 0; list < 2; ++list) m = std::max(m, g->nHalo[side][list]);
+  return m;
 }
 
 // Pending SetNode edits go up on the instance's stream, which is then
@@ -950,9 +1087,24 @@ static cudaStream_t stream_or(Gpu* g, void* stream) {
   return stream ? static_cast<cudaStream_t>(stream) : g->stream;
 }
 
+// The halo slot list a list slab packs (pack = true) or unpacks through
+// `side` in `phase`, or -1 if that face has no halo.
+static int list_halo_list(Gpu* g, int side, int phase, bool pack) {
+  const int list = (phase == 0) == pack ? 0 : 1;
+  return g->nHalo[side][list] < 0 ? -1 : list;
+}
+
 int lbm_aa_halo_pack(KernelData* kd, int side, int phase, double* buf, void* stream) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
-  if (g->kind != kAa || side < 0 || side > 1 || phase < 0 || phase > 1) return -1;
+  if (side < 0 || side > 1 || phase < 0 || phase > 1) return -1;
+  if (g->listSlab) {
+    const int list = list_halo_list(g, side, phase, true);
+    if (list < 0) return -1;
+    sync_upload(g);
+    lbm::slot_gather(g->dF, g->dHalo[side][list], g->nHalo[side][list], buf, stream_or(g, stream));
+    return (int)cudaGetLastError();
+  }
+  if (g->kind != kAa) return -1;
   sync_upload(g);
   lbm::aa_halo_pack(aa_args(g), side, phase, buf, stream_or(g, stream));
   return (int)cudaGetLastError();
@@ -960,7 +1112,15 @@ int lbm_aa_halo_pack(KernelData* kd, int side, int phase, double* buf, void* str
 
 int lbm_aa_halo_unpack(KernelData* kd, int side, int phase, const double* buf, void* stream) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
-  if (g->kind != kAa || side < 0 || side > 1 || phase < 0 || phase > 1) return -1;
+  if (side < 0 || side > 1 || phase < 0 || phase > 1) return -1;
+  if (g->listSlab) {
+    const int list = list_halo_list(g, side, phase, false);
+    if (list < 0) return -1;
+    sync_upload(g);
+    lbm::slot_scatter(g->dF, g->dHalo[side][list], g->nHalo[side][list], buf, stream_or(g, stream));
+    return (int)cudaGetLastError();
+  }
+  if (g->kind != kAa) return -1;
   sync_upload(g);
   lbm::aa_halo_unpack(aa_args(g), side, phase, buf, stream_or(g, stream));
   return (int)cudaGetLastError();
@@ -968,11 +1128,21 @@ int lbm_aa_halo_unpack(KernelData* kd, int side, int phase, const double* buf, v
 
 int lbm_aa_slab_step(KernelData* kd, CaseData* cd, int half, void* stream) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
-  if (g->kind != kAa || half < 0 || half > 1) return -1;
+  if (half < 0 || half > 1 || (g->kind != kAa && !g->listSlab)) return -1;
   sync_upload(g);
   const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
-  const lbm::AaArgs a = aa_args(g);
   const cudaStream_t s = stream_or(g, stream);
+  if (g->listSlab) {
+    const lbm::ListArgs la = list_args(g);
+    if (half == 0) {
+      lbm::list_even_fp64(la, t, s);
+    } else {
+      lbm::list_odd_fp64(la, t, s);
+      g->iteration += 2;
+    }
+    return (int)cudaGetLastError();
+  }
+  const lbm::AaArgs a = aa_args(g);
   if (half == 0) {
     lbm::aa_even_fp64(a, t, s);
   } else {

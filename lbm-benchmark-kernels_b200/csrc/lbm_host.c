@@ -245,6 +245,166 @@ int lbmh_list_build(const LatticeDesc *ld, int pull, const int blk[3], int nCell
 }
 
 /* ------------------------------------------------------------------------ */
+/* One x-slab [x0, x1) of a list-AA lattice split along x (no counterpart in
+ * the reference, whose list kernels address one array). Owned nodes are the
+ * slab's fluid cells in lbmh_list_build's blocked numbering over the slab;
+ * ghost nodes follow them: the fluid cells of the neighbouring slabs that an
+ * owned node's link reaches, in the order the owned nodes first reach them.
+ * Links follow the whole lattice's rule, so an owned node's adjacency equals
+ * its adjacency in the undivided lattice with remote nodes replaced by ghosts. */
+
+/* Target of link d (push model) of fluid cell (x, y, z) under the rule of
+ * lbmh_list_build: 1 and the cell in q if the link reaches a fluid cell, 0 if
+ * it bounces back. */
+static int list_link_target(const LatticeDesc *ld, int x, int y, int z, int d, int q[3])
+{
+	const int *dims = ld->Dims;
+	const int per[3] = { ld->PeriodicX, ld->PeriodicY, ld->PeriodicZ };
+	q[0] = x + kVel[d].x; q[1] = y + kVel[d].y; q[2] = z + kVel[d].z;
+	int out = 0, crossPer = 0;
+	for (int a = 0; a < 3; ++a) {
+		const int o = q[a] < 0 || q[a] >= dims[a];
+		out |= o;
+		crossPer |= o && per[a];
+	}
+	if (crossPer) {
+		for (int a = 0; a < 3; ++a) q[a] = q[a] < 0 ? dims[a] - 1 : (q[a] >= dims[a] ? 0 : q[a]);
+		out = 0;
+	}
+	if (out) return 0;
+	return ld->Lattice[lbmh_lidx(dims, q[0], q[1], q[2])] != LAT_CELL_OBSTACLE;
+}
+
+void lbmh_list_slab_free(LbmhListSlab *s)
+{
+	free(s->grid); free(s->adj);
+	for (int k = 0; k < 2; ++k) { free(s->own[k]); free(s->ghost[k]); }
+	memset(s, 0, sizeof(*s));
+}
+
+/* Visits the slab's fluid cells in the owned numbering order. */
+#define SLAB_CELLS_BEGIN(ld, x0, x1, bx, by, bz)                                   \
+	for (int X0 = (x0); X0 < (x1); X0 += (bx))                                     \
+	for (int Y0 = 0; Y0 < (ld)->Dims[1]; Y0 += (by))                               \
+	for (int Z0 = 0; Z0 < (ld)->Dims[2]; Z0 += (bz)) {                             \
+		const int X1 = X0 + (bx) < (x1) ? X0 + (bx) : (x1);                        \
+		const int Y1 = Y0 + (by) < (ld)->Dims[1] ? Y0 + (by) : (ld)->Dims[1];      \
+		const int Z1 = Z0 + (bz) < (ld)->Dims[2] ? Z0 + (bz) : (ld)->Dims[2];      \
+		for (int x = X0; x < X1; ++x)                                              \
+		for (int y = Y0; y < Y1; ++y)                                              \
+		for (int z = Z0; z < Z1; ++z) {                                            \
+			if ((ld)->Lattice[lbmh_lidx((ld)->Dims, x, y, z)] == LAT_CELL_OBSTACLE) continue;
+#define SLAB_CELLS_END }}
+
+int lbmh_list_slab_build(const LatticeDesc *ld, int x0, int x1, const int halo[2], const int blk[3],
+                         const char *pad, LbmhListSlab *s)
+{
+	const int nx = ld->Dims[0], ny = ld->Dims[1], nz = ld->Dims[2];
+	const int L = x1 - x0;
+	memset(s, 0, sizeof(*s));
+	if (x0 < 0 || x1 > nx || L < 1) return -1;
+	if ((halo[0] || halo[1]) && L == nx) return -1;
+	const int bx = blk && blk[0] > 0 ? blk[0] : L;
+	const int by = blk && blk[1] > 0 ? blk[1] : ny;
+	const int bz = blk && blk[2] > 0 ? blk[2] : nz;
+	const long plane = (long)ny * nz;
+	const int xLo = (x0 - 1 + nx) % nx, xHi = x1 % nx;
+	s->L = L;
+	s->grid = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)L * plane);
+	int *gmap[2];
+	gmap[0] = (int *)malloc(sizeof(int) * (size_t)plane);
+	gmap[1] = xHi == xLo ? gmap[0] : (int *)malloc(sizeof(int) * (size_t)plane);
+	int rc = 0;
+	if (!s->grid || !gmap[0] || !gmap[1]) { rc = -3; goto done; }
+	for (long i = 0; i < (long)L * plane; ++i) s->grid[i] = 0xffffffffu;
+	for (long i = 0; i < plane; ++i) gmap[0][i] = gmap[1][i] = -1;
+	const int ldims[3] = { L, ny, nz };
+
+	uint32_t count = 0;
+	SLAB_CELLS_BEGIN(ld, x0, x1, bx, by, bz)
+		s->grid[lbmh_lidx(ldims, x - x0, y, z)] = count++;
+	SLAB_CELLS_END
+	s->nOwned = (int)count;
+
+	/* ghosts, in the order the owned nodes first reach them */
+	int nGhost = 0;
+	SLAB_CELLS_BEGIN(ld, x0, x1, bx, by, bz)
+		for (int d = 0; d < 18; ++d) {
+			int q[3];
+			if (!list_link_target(ld, x, y, z, d, q) || (q[0] >= x0 && q[0] < x1)) continue;
+			const int side = kVel[d].x < 0 ? 0 : 1;
+			if (!halo[side]) { rc = -2; goto done; }
+			int *g = &gmap[side][(long)q[2] * ny + q[1]];
+			if (*g < 0) *g = nGhost++;
+		}
+	SLAB_CELLS_END
+	s->nGhost = nGhost;
+	s->nCells = lbmh_pad_cells(s->nOwned + nGhost, (int)sizeof(double), pad);
+	if (s->nCells < 0) { rc = -4; goto done; }
+	if ((uint64_t)19 * (uint64_t)s->nCells >= (1ull << 32)) { rc = -5; goto done; }
+	const uint32_t nc = (uint32_t)s->nCells;
+
+	s->adj = (uint32_t *)malloc(sizeof(uint32_t) * 18 * (size_t)(s->nOwned > 0 ? s->nOwned : 1));
+	if (!s->adj) { rc = -3; goto done; }
+	SLAB_CELLS_BEGIN(ld, x0, x1, bx, by, bz)
+		const uint32_t self = s->grid[lbmh_lidx(ldims, x - x0, y, z)];
+		uint32_t *row = s->adj + (size_t)self * 18;
+		for (int d = 0; d < 18; ++d) {
+			int q[3];
+			uint32_t dst = (uint32_t)kVel[d].inv * nc + self; /* bounce back */
+			if (list_link_target(ld, x, y, z, d, q)) {
+				if (q[0] >= x0 && q[0] < x1)
+					dst = (uint32_t)d * nc + s->grid[lbmh_lidx(ldims, q[0] - x0, q[1], q[2])];
+				else
+					dst = (uint32_t)d * nc + (uint32_t)(s->nOwned + gmap[kVel[d].x < 0 ? 0 : 1][(long)q[2] * ny + q[1]]);
+			}
+			row[d] = dst;
+		}
+	SLAB_CELLS_END
+
+	/* halo slot lists. Side 0 faces x0, side 1 faces x1 - 1. ghost[side]:
+	 * the ghost slots this slab's face cells reach through that face; own[side]:
+	 * the owned slots the neighbour's face cells reach through it. Both are
+	 * in the order (z, y, d) of the reaching cell and link, so a slab's ghost
+	 * list and its neighbour's own list for the shared face match entry for
+	 * entry. */
+	for (int side = 0; side < 2; ++side) {
+		if (!halo[side]) continue;
+		s->ghost[side] = (uint32_t *)malloc(sizeof(uint32_t) * 5 * (size_t)plane);
+		s->own[side] = (uint32_t *)malloc(sizeof(uint32_t) * 5 * (size_t)plane);
+		if (!s->ghost[side] || !s->own[side]) { rc = -3; goto done; }
+		const int xf = side ? x1 - 1 : x0;        /* this slab's face plane */
+		const int xn = side ? xHi : xLo;          /* the neighbour's face plane */
+		const int toward = side ? 1 : -1;
+		long ng = 0, no = 0;
+		for (int z = 0; z < nz; ++z)
+		for (int y = 0; y < ny; ++y) {
+			if (ld->Lattice[lbmh_lidx(ld->Dims, xf, y, z)] != LAT_CELL_OBSTACLE)
+				for (int d = 0; d < 18; ++d) {
+					int q[3];
+					if (kVel[d].x != toward || !list_link_target(ld, xf, y, z, d, q)) continue;
+					if (q[0] >= x0 && q[0] < x1) continue;
+					s->ghost[side][ng++] = (uint32_t)d * nc + (uint32_t)(s->nOwned + gmap[side][(long)q[2] * ny + q[1]]);
+				}
+			if (ld->Lattice[lbmh_lidx(ld->Dims, xn, y, z)] != LAT_CELL_OBSTACLE)
+				for (int d = 0; d < 18; ++d) {
+					int q[3];
+					if (kVel[d].x != -toward || !list_link_target(ld, xn, y, z, d, q)) continue;
+					if (q[0] < x0 || q[0] >= x1) continue;
+					s->own[side][no++] = (uint32_t)d * nc + s->grid[lbmh_lidx(ldims, q[0] - x0, q[1], q[2])];
+				}
+		}
+		s->nGhostSlots[side] = ng;
+		s->nOwnSlots[side] = no;
+	}
+done:
+	if (gmap[1] != gmap[0]) free(gmap[1]);
+	free(gmap[0]);
+	if (rc) lbmh_list_slab_free(s);
+	return rc;
+}
+
+/* ------------------------------------------------------------------------ */
 /* AA link words. A link d of fluid cell x is "reversed" when x + c_d is not a
  * fluid node reached directly or through a periodic wrap: an obstacle inside
  * the domain, an obstacle reached through a wrap, or a non-periodic exit. The

@@ -33,6 +33,31 @@ int lbmh_pad_cells(int nCells, int pdfBytes, const char *padStr);
 int lbmh_list_build(const LatticeDesc *ld, int pull, const int blk[3], int nCells,
                     uint32_t *grid, uint32_t *coords, uint32_t *adj);
 
+/* One x-slab [x0, x1) of a list-AA (push adjacency) lattice split along x:
+ * owned nodes (the slab's fluid cells, blocked numbering over the slab) then
+ * ghost nodes (fluid cells of the neighbouring slabs that owned links
+ * reach); adj indexes f[d * nCells + node] like lbmh_list_build's. Halo
+ * lists per side (0: the x0 face, 1: the x1 - 1 face): ghost[side] = the
+ * ghost slots that this slab's face cells reach through the face, own[side]
+ * = the owned slots that the neighbour's face cells reach through it, both
+ * in (z, y, link) order of the reaching cell, so that one slab's ghost list
+ * and the neighbour's own list for their shared face pair up entry by entry. */
+typedef struct {
+	int L, nOwned, nGhost, nCells;
+	uint32_t *grid;       /* L * nY * nZ slab cells (x fastest); obstacles 0xffffffff */
+	uint32_t *adj;        /* nOwned * 18 */
+	uint32_t *own[2], *ghost[2];
+	long nOwnSlots[2], nGhostSlots[2];
+} LbmhListSlab;
+
+/* Builds the slab layout (halo[side] = 1: that face has a neighbour slab).
+ * Returns 0; -1 bad range (or a halo on a slab that spans the lattice);
+ * -2 a link leaves through a face without a halo; -3 allocation failure;
+ * -4 malformed padding string; -5 more PDFs than 32-bit indices address. */
+int lbmh_list_slab_build(const LatticeDesc *ld, int x0, int x1, const int halo[2], const int blk[3],
+                         const char *pad, LbmhListSlab *s);
+void lbmh_list_slab_free(LbmhListSlab *s);
+
 /* Link words of the full-array AA layout: for every cell of the padded
  * (nX+2) x (nY+2) x pitch array, bit 31 = fluid cell, bit d = link d of the
  * cell does not reach a fluid node (wall or open face). Ghost and pad cells

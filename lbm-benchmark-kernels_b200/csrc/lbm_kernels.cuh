@@ -1,6 +1,7 @@
 // lbm_kernels.cuh -- argument blocks and launchers of the sm_100a D3Q19 TRT
 // time-step kernels (definitions in lbm_kernels_fp64.cu).
 #pragma once
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 
@@ -74,7 +75,27 @@ struct ListArgs {
   long long nCells;
   int nFluid;
   int* err;       // device error word (bounded waits)
+  int prefetch;   // tiles ahead whose adjacency a block prefetches into L2 (0: none)
 };
+
+// The prefetch distance of a launch of `kernel` (threads per block): its
+// resident blocks across the device, so that a block prefetches the tile of
+// the block that takes its place when the first wave retires. `ahead` caches
+// it per launcher; `enabled` false gives 0 (no prefetch).
+template <class K>
+int prefetch_distance(std::atomic<int>& ahead, K kernel, int threads, bool enabled) {
+  if (!enabled) return 0;
+  int v = ahead.load(std::memory_order_acquire);
+  if (v <= 0) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0);
+    v = sms * per;
+    ahead.store(v, std::memory_order_release);
+  }
+  return v;
+}
 
 // Reduced-storage list AA (lbm_kernels_lp.cu): PDFs stored as FP32 or as
 // scaled FP16 deviations from the weights, collision in FP32.
@@ -93,6 +114,7 @@ struct ListArgsLp {
   long long nCells;
   int nFluid;
   int* err;
+  int prefetch;  // as ListArgs::prefetch
 };
 
 // List layout built on the device (lbm_build.cu): numbering into grid (one
@@ -101,6 +123,11 @@ struct ListArgsLp {
 long long list_build_device(const int* mask, const int dims[3], const int periodic[3], int pull, const int blk[3],
                             int nCells, uint32_t* grid, uint32_t* adj, long long adjCap, cudaStream_t s,
                             const char** err);
+
+// Halo messages of a list slab: buf[k] = f[idx[k]] (gather) and
+// f[idx[k]] = buf[k] (scatter) for k < n.
+void slot_gather(const double* f, const uint32_t* idx, long long n, double* buf, cudaStream_t s);
+void slot_scatter(double* f, const uint32_t* idx, long long n, const double* buf, cudaStream_t s);
 
 // Launchers (stream-ordered, no synchronisation).
 void list_even_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s);

@@ -2,6 +2,7 @@
 // in HBM as FP32 or FP16 deviations from the lattice weights (lbm_store.cuh),
 // with the collision evaluated in FP32 (FMA contraction allowed in this file).
 // Bytes per fluid-lattice update: even 19*2*s, odd 19*2*s + 72 (s = 4 or 2).
+#include <atomic>
 #include <type_traits>
 
 #include "lbm_bulk.cuh"
@@ -117,6 +118,9 @@ __device__ __forceinline__ bool stage_adj_tile_lp(const ListArgsLp& a, uint32_t*
     mbar_init(bar, 1);
     mbar_arrive_expect_tx(bar, kListTile * QM * 4);
     bulk_g2s(sadj, a.adj + static_cast<size_t>(blockIdx.x) * kListTile * QM, kListTile * QM * 4, bar);
+    const unsigned ahead = blockIdx.x + a.prefetch;
+    if (a.prefetch > 0 && ahead < gridDim.x)
+      bulk_prefetch_l2(a.adj + static_cast<size_t>(ahead) * kListTile * QM, kListTile * QM * 4);
   }
   __syncthreads();
   if (!mbar_wait_bounded(bar, 0)) {
@@ -162,17 +166,19 @@ constexpr int kEvenStageBytes = 2048, kEvenStages = 2, kEvenBlocksPerSM = 2;
 template <class St>
 static void launch_even_staged(const ListArgsLp& a, const Trt<float>& t, cudaStream_t s) {
   constexpr int kMaxDevices = 64;
-  static int grid[kMaxDevices] = {0};
+  static std::atomic<int> grid[kMaxDevices];
   constexpr size_t smem = (size_t)kEvenStages * Q * kEvenStageBytes;
   auto kern = k_list_even_staged<St, kEvenStageBytes, kEvenStages>;
   int dev = 0;
   cudaGetDevice(&dev);
-  int& g = grid[dev < kMaxDevices ? dev : 0];
-  if (g == 0 || dev >= kMaxDevices) {
+  int g = dev < kMaxDevices ? grid[dev].load(std::memory_order_acquire) : 0;
+  if (g == 0) {
+    // idempotent: concurrent first launches on a device set the same values
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     g = sms * kEvenBlocksPerSM;
+    if (dev < kMaxDevices) grid[dev].store(g, std::memory_order_release);
   }
   kern<<<g, 256, smem, s>>>(a, t);
 }
@@ -190,10 +196,15 @@ void list_even_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStr
 
 void list_odd_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s) {
   if (a.nFluid <= 0) return;
-  if (storage == kStoreF16)
-    k_list_odd_lp<StoreF16><<<lp_blocks(a), kListTile, 0, s>>>(a, t);
-  else
-    k_list_odd_lp<StoreF32><<<lp_blocks(a), kListTile, 0, s>>>(a, t);
+  static std::atomic<int> ahead16{0}, ahead32{0};
+  ListArgsLp b = a;
+  if (storage == kStoreF16) {
+    b.prefetch = prefetch_distance(ahead16, k_list_odd_lp<StoreF16>, kListTile, a.prefetch != 0);
+    k_list_odd_lp<StoreF16><<<lp_blocks(b), kListTile, 0, s>>>(b, t);
+  } else {
+    b.prefetch = prefetch_distance(ahead32, k_list_odd_lp<StoreF32>, kListTile, a.prefetch != 0);
+    k_list_odd_lp<StoreF32><<<lp_blocks(b), kListTile, 0, s>>>(b, t);
+  }
 }
 
 }  // namespace lbm

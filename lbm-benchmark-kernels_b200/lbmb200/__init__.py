@@ -296,6 +296,15 @@ class Instance:
     def density(self):
         return lib().lbm_density(self.kdp, ctypes.byref(self.lattice.desc))
 
+    def moments(self):
+        """lbm_b200_instance_moments: FP64 (sum rho, sum j_x, sum j_y, sum j_z)
+        over the instance's fluid nodes (FP64 list kernels)."""
+        out = (ctypes.c_double * 4)()
+        rc = lib().lbm_b200_instance_moments(self.kdp, out)
+        if rc:
+            raise RuntimeError("moments failed (%d): %s" % (rc, lib().lbm_b200_last_error().decode()))
+        return tuple(out)
+
     def list_layout(self):
         g = ctypes.POINTER(ctypes.c_uint32)()
         a = ctypes.POINTER(ctypes.c_uint32)()

@@ -46,6 +46,16 @@ class Ranks:
     def sum(self, v):
         return self._reduce(v, self.dist.ReduceOp.SUM if self.dist else None)
 
+    def sum_vec(self, values):
+        """Element-wise FP64 sum over ranks of a short vector (conservation
+        sums of a decomposed lattice)."""
+        vals = [float(v) for v in values]
+        if self.dist is None:
+            return vals
+        t = self.torch.tensor(vals, dtype=self.torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return [float(v) for v in t.tolist()]
+
     def share(self, items):
         """This rank's share of a list (round robin)."""
         return list(items)[self.rank::self.world]

@@ -1,16 +1,23 @@
-"""Command-line run of one full-array AA lattice split into x-slabs, one slab
+"""Command-line run of one AA-pattern lattice split into x-slabs, one slab
 per GPU, halo messages through torch.distributed (NCCL):
 
     python -m torch.distributed.run --nproc-per-node 4 --master-addr 127.0.0.1 \\
         -m lbmb200.slabrun --dims 1024x256x256 --geometry fluid --periodic xyz --pairs 50
+    ... -m lbmb200.slabrun --layout list --dims 512x256x256 \\
+        --geometry spheres:20251203:0.4:6:12 --pairs 50
 
 (run with lbm-benchmark-kernels_b200 on the Python path). Every rank builds the
-same lattice, takes its slab, and runs `pairs` even/odd step pairs; rank 0
-prints the aggregate MFLUP/s (device-timed per rank with CUDA events, max over
-ranks). With one process, the lattice runs as one slab without halos.
+same lattice, takes its slab -- full array (cuda-aa-soa kernels) or fluid-node
+list (cuda-list-aa-pv-soa kernels) -- and runs `pairs` even/odd step pairs;
+rank 0 prints the aggregate MFLUP/s (device-timed per rank with CUDA events,
+max over ranks). List slabs also report the FP64 conservation sums of the
+whole lattice (per-slab sums all-reduced) and the permeability they give.
+With one process, the lattice runs as one slab without halos.
 """
 import argparse
 import json
+
+import numpy as np
 
 
 def main(argv=None):
@@ -22,6 +29,7 @@ def main(argv=None):
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--omega", type=float, default=1.0)
     p.add_argument("--lambda", dest="lam", default="3/16")
+    p.add_argument("--layout", default="full", choices=("full", "list"))
     a = p.parse_args(argv)
 
     import torch
@@ -41,7 +49,9 @@ def main(argv=None):
         lo, hi = sl.halo_flags(ranks.rank, ranks.world, ring)
         lbmb200.lib().lbm_b200_set_device(ranks.local)
         torch.cuda.set_device(ranks.local)
-        slab = sl.Slab(lat, x0, x1, lo, hi, kernel_args=["-lambda", a.lam])
+        slab = sl.Slab(lat, x0, x1, lo, hi, kernel_args=["-lambda", a.lam], layout=a.layout)
+        if a.layout == "list":
+            slab.inst.set_field(np.broadcast_to(lbmb200.W, (slab.local.mask.size, 19)))
         # an explicit stream, current for torch.distributed too: kernels,
         # packs, the library's sends/receives and unpacks run in one order
         work = torch.cuda.Stream()
@@ -60,10 +70,16 @@ def main(argv=None):
         torch.cuda.synchronize()
         ms = ranks.max(e0.elapsed_time(e1))
         nodes = ranks.sum(slab.local.n_fluid)
+        rec = {"dims": dims, "geometry": a.geometry, "layout": a.layout, "ranks": ranks.world,
+               "fluid_nodes": nodes, "pairs": a.pairs, "ms": round(ms, 3),
+               "mflups": round(nodes * 2 * a.pairs / (ms / 1e3) / 1e6, 1)}
+        if a.layout == "list":
+            from lbmb200.porous import permeability
+            rho, jx, jy, jz = ranks.sum_vec(slab.inst.moments())
+            rec.update({"sum_rho": rho, "sum_jx": jx, "sum_jy": jy, "sum_jz": jz,
+                        "permeability": permeability(jx, nodes, dims[0] * dims[1] * dims[2], a.omega, cd.XForce)})
         if ranks.rank == 0:
-            print(json.dumps({"dims": dims, "geometry": a.geometry, "ranks": ranks.world, "fluid_nodes": nodes,
-                              "pairs": a.pairs, "ms": round(ms, 3),
-                              "mflups": round(nodes * 2 * a.pairs / (ms / 1e3) / 1e6, 1)}))
+            print(json.dumps(rec))
         slab.close()
     finally:
         ranks.close()

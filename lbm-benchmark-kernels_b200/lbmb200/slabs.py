@@ -1,6 +1,9 @@
-"""One full-array AA lattice split into x-slabs: one slab per GPU (one process
+"""One AA-pattern lattice split into x-slabs: one slab per GPU (one process
 per GPU, torch.distributed for the halo messages), or several slabs in one
 process on one GPU (tests, and the same arithmetic without a second GPU).
+Two layouts: the full array (cuda-aa-soa kernels) and the fluid-node list
+(cuda-list-aa-pv-soa kernels, FP64), whose slabs keep ghost nodes for the
+neighbours' fluid cells that their links reach.
 
 A step pair of the AA pattern on a slab:
 
@@ -16,7 +19,8 @@ A step pair of the AA pattern on a slab:
 Every slot is read and written by exactly one cell in the odd step, so after
 the pair the slabs hold the whole lattice's state bit for bit (tested against
 the single-instance kernel). Messages are 5 x nY x nZ doubles per face and
-phase (lbm_aa_halo_count).
+phase for full-array slabs, one double per link through the face for list
+slabs (``Slab.message``).
 
 Transports: ``LocalTransport`` (all slabs in this process: device-to-device
 through shared device buffers, every operation on one stream) and
@@ -66,7 +70,14 @@ def _sigs(L):
         L.lbm_aa_slab_init.restype = ctypes.POINTER(KernelData)
         L.lbm_aa_slab_init.argtypes = [ctypes.POINTER(LatticeDesc), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, ctypes.POINTER(Parameters)]
+        L.lbm_aa_list_slab_init.restype = ctypes.POINTER(KernelData)
+        L.lbm_aa_list_slab_init.argtypes = L.lbm_aa_slab_init.argtypes
         L.lbm_aa_halo_count.restype = ctypes.c_longlong
+        L.lbm_aa_halo_message.restype = ctypes.c_longlong
+        L.lbm_aa_halo_message.argtypes = [ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.lbm_aa_list_slab_layout.argtypes = [ctypes.POINTER(LatticeDesc), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ctypes.POINTER(Parameters),
+                                              ctypes.POINTER(ctypes.c_longlong)] + [ctypes.c_void_p] * 6
         for name in ("lbm_aa_halo_pack", "lbm_aa_halo_unpack"):
             getattr(L, name).argtypes = [ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                          ctypes.c_void_p]
@@ -80,28 +91,42 @@ def _ptr(buf):
     return buf.data_ptr() if hasattr(buf, "data_ptr") else int(buf)
 
 
-class Slab:
-    """The x range [x0, x1) of `lattice` as an AA instance on the current
-    device (cuda-aa-soa kernels; kernel_args as for its Init)."""
+def _params(kernel_args):
+    args = [a.encode() for a in kernel_args]
+    argv = (ctypes.c_char_p * max(1, len(args)))(*args)
+    p = Parameters()
+    p.nArgs, p.Args, p.nKernelArgs, p.KernelArgs = 0, None, len(args), argv
+    return p, argv
 
-    def __init__(self, lattice, x0, x1, halo_lo, halo_hi, kernel_args=()):
+
+class Slab:
+    """The x range [x0, x1) of `lattice` as an AA-pattern instance on the
+    current device: layout "full" (cuda-aa-soa kernels) or "list"
+    (cuda-list-aa-pv-soa kernels, FP64); kernel_args as for the kernel's
+    Init."""
+
+    def __init__(self, lattice, x0, x1, halo_lo, halo_hi, kernel_args=(), layout="full"):
+        if layout not in ("full", "list"):
+            raise ValueError("layout must be 'full' or 'list'")
         self.L = _sigs(lib())
         nx, ny, nz = lattice.dims
-        self.x0, self.x1 = x0, x1
+        self.x0, self.x1, self.layout = x0, x1, layout
         mask = lattice.mask.reshape(nz, ny, nx)[:, :, x0:x1]
         self.local = Lattice(mask.reshape(-1), (x1 - x0, ny, nz), lattice.periodic, "slab")
-        args = [a.encode() for a in kernel_args]
-        self._argv = (ctypes.c_char_p * max(1, len(args)))(*args)
-        p = Parameters()
-        p.nArgs, p.Args, p.nKernelArgs, p.KernelArgs = 0, None, len(args), self._argv
+        p, self._argv = _params(kernel_args)
         self._global = lattice  # keeps the lattice's mask alive for the call
-        kdp = self.L.lbm_aa_slab_init(ctypes.byref(lattice.desc), x0, x1, int(halo_lo), int(halo_hi),
-                                      ctypes.byref(p))
+        init = self.L.lbm_aa_slab_init if layout == "full" else self.L.lbm_aa_list_slab_init
+        kdp = init(ctypes.byref(lattice.desc), x0, x1, int(halo_lo), int(halo_hi), ctypes.byref(p))
         if not kdp:
             raise RuntimeError("slab init failed: %s" % self.L.lbm_b200_last_error().decode())
         self.inst = Instance(None, self.local, kdp)
         self.kdp = kdp
         self.count = int(self.L.lbm_aa_halo_count(kdp))
+
+    def message(self, side, phase, send):
+        """Doubles this slab sends (send=True) or receives through `side` in
+        `phase` (-1: no halo on that face)."""
+        return int(self.L.lbm_aa_halo_message(self.kdp, int(side), int(phase), int(bool(send))))
 
     def step(self, cd, half, stream=None):
         rc = self.L.lbm_aa_slab_step(self.kdp, ctypes.byref(cd), int(half), stream)
@@ -124,6 +149,13 @@ class Slab:
             self.kdp = None
 
 
+def message(slab, side, phase, send):
+    """Length of a slab's message through `side` in `phase`: the slab's own
+    ``message`` method, else its fixed ``count``."""
+    m = getattr(slab, "message", None)
+    return m(side, phase, send) if m else slab.count
+
+
 class LocalTransport:
     """All slabs of the lattice in this process, on one device: messages go
     through device buffers, and every step, pack and unpack is enqueued on
@@ -138,7 +170,12 @@ class LocalTransport:
         n = len(slabs)
         # faces between slab r (side 1) and its right-hand neighbour (side 0)
         self.faces = [(r, (r + 1) % n) for r in range(n) if neighbours(r, n, ring)[1] is not None]
-        self.bufs = {f: (alloc(slabs[f[0]].count), alloc(slabs[f[0]].count)) for f in self.faces}
+        for (r, q) in self.faces:
+            for phase in (0, 1):
+                if (message(slabs[r], 1, phase, True) != message(slabs[q], 0, phase, False)
+                        or message(slabs[q], 0, phase, True) != message(slabs[r], 1, phase, False)):
+                    raise ValueError("slabs %d and %d disagree on their shared face's messages" % (r, q))
+        self.bufs = {f: (alloc(max(1, slabs[f[0]].count)), alloc(max(1, slabs[f[1]].count))) for f in self.faces}
 
     def exchange(self, phase):
         for (r, q) in self.faces:
@@ -158,29 +195,57 @@ class DistTransport:
     def __init__(self, slab, rank, world, ring, dist, make_buf, stream=None):
         self.slab, self.dist, self.stream = slab, dist, stream
         self.left, self.right = neighbours(rank, world, ring)
-        self.send = {s: make_buf(slab.count) for s in (0, 1)}
-        self.recv = {s: make_buf(slab.count) for s in (0, 1)}
+        # one buffer per face and direction; each phase's message is a prefix
+        self.send = {s: make_buf(max(1, max(message(slab, s, p, True) for p in (0, 1)))) for s in (0, 1)}
+        self.recv = {s: make_buf(max(1, max(message(slab, s, p, False) for p in (0, 1)))) for s in (0, 1)}
 
     def exchange(self, phase, sync=None):
         d = self.dist
-        for side in (1, 0):
-            if (self.right if side else self.left) is not None:
-                self.slab.pack(side, phase, self.send[side], self.stream)
+        faces = [s for s in (1, 0) if (self.right if s else self.left) is not None]
+        out = {s: self.send[s][:message(self.slab, s, phase, True)] for s in faces}
+        inc = {s: self.recv[s][:message(self.slab, s, phase, False)] for s in faces}
+        for side in faces:
+            self.slab.pack(side, phase, out[side], self.stream)
         if sync:
             sync()  # the packed buffers are complete before the library sends them
         ops = []
         for side, peer in ((1, self.right), (0, self.left)):
             if peer is not None:
-                ops.append(d.P2POp(d.isend, self.send[side], peer))
+                ops.append(d.P2POp(d.isend, out[side], peer))
         for side, peer in ((0, self.left), (1, self.right)):
             if peer is not None:
-                ops.append(d.P2POp(d.irecv, self.recv[side], peer))
+                ops.append(d.P2POp(d.irecv, inc[side], peer))
         if ops:
             for req in d.batch_isend_irecv(ops):
                 req.wait()
         for side in (0, 1):
             if (self.right if side else self.left) is not None:
-                self.slab.unpack(side, phase, self.recv[side], self.stream)
+                self.slab.unpack(side, phase, inc[side], self.stream)
+
+
+def list_slab_layout(lattice, x0, x1, halo_lo, halo_hi, kernel_args=()):
+    """The layout of a list slab, built on the host (no CUDA call): a dict
+    with n_owned, n_ghost, n_cells, grid (slab cells, x fastest), adj
+    (n_owned x 18) and the slot lists own / ghost per side (None: no halo)."""
+    L = _sigs(lib())
+    nx, ny, nz = lattice.dims
+    p, argv = _params(kernel_args)
+    counts = (ctypes.c_longlong * 7)()
+    args = (ctypes.byref(lattice.desc), x0, x1, int(halo_lo), int(halo_hi), ctypes.byref(p), counts)
+    rc = L.lbm_aa_list_slab_layout(*args, None, None, None, None, None, None)
+    if rc:
+        raise RuntimeError("list slab layout failed (%d): %s" % (rc, L.lbm_b200_last_error().decode()))
+    n_owned = counts[0]
+    grid = np.zeros((x1 - x0) * ny * nz, dtype=np.uint32)
+    adj = np.zeros(max(1, n_owned) * 18, dtype=np.uint32)
+    lists = [np.zeros(max(1, counts[3 + k]), dtype=np.uint32) for k in range(4)]
+    ptr = [a.ctypes.data for a in [grid, adj] + lists]
+    rc = L.lbm_aa_list_slab_layout(*args, *ptr)
+    if rc:
+        raise RuntimeError("list slab layout failed (%d)" % rc)
+    cut = [lists[k][:counts[3 + k]] if counts[3 + k] >= 0 else None for k in range(4)]
+    return {"n_owned": n_owned, "n_ghost": counts[1], "n_cells": counts[2], "grid": grid,
+            "adj": adj[: n_owned * 18], "own": (cut[0], cut[2]), "ghost": (cut[1], cut[3])}
 
 
 def step_pairs(slabs, transport, cd, pairs, stream=None):

@@ -576,6 +576,45 @@ static void list_odd(orc_state_t *s, const trt_t *t)
 	}
 }
 
+/* One half of a list AA step pair on a caller-supplied layout (nodes
+ * [0, n_nodes) of f[d * n_cells + node], push adjacency adj[node * 18 + d]),
+ * for checking decomposed runs whose slabs hold ghost nodes past n_nodes.
+ * The arithmetic is list_even / list_odd above. The reference's per-step body
+ * force (src/Kernel.c:759-803, add_body_force) is added to each slot once, at
+ * the access that follows it: the even step's force when the odd step loads a
+ * value, the odd step's force when it stores one (a slot it bounces into
+ * carries the force of the inverse direction). That is the same single
+ * addition per slot as the separate pass, so every complete pair leaves the
+ * bits orc_run leaves, and a slot that another slab updates between the two
+ * halves receives its force from the node that reads it. */
+int orc_list_aa_half(int odd, int n_nodes, int n_cells, const uint32_t *adj, double *f,
+                     double omega, double lambda, double xforce)
+{
+	const trt_t t = trt_make(omega, lambda);
+	double ft[Q];
+	for (int d = 0; d < Q; ++d) ft[d] = force_term(d, xforce);
+	const size_t nc = (size_t)n_cells;
+	for (int n = 0; n < n_nodes; ++n) {
+		double p[Q], o[Q];
+		if (!odd) {
+			for (int d = 0; d < Q; ++d) p[d] = f[d * nc + n];
+			trt_collide(&t, p, o);
+			for (int d = 0; d < Q; ++d) f[INV[d] * nc + n] = o[d];
+			continue;
+		}
+		const uint32_t *a = adj + (size_t)n * QM;
+		for (int d = 0; d < QM; ++d) p[d] = f[a[INV[d]]] + ft[d];
+		p[DC] = f[DC * nc + n] + ft[DC];
+		trt_collide(&t, p, o);
+		for (int d = 0; d < QM; ++d) {
+			const int bounce = a[d] == (uint32_t)(INV[d] * nc + n);
+			f[a[d]] = o[d] + (bounce ? ft[INV[d]] : ft[d]);
+		}
+		f[DC * nc + n] = o[DC] + ft[DC];
+	}
+	return 0;
+}
+
 /* List pull (src/BenchKernelD3Q19ListPullSplitNt1SScalar.h): gather through the
  * pull adjacency from the source grid, write the destination grid. */
 static void list_pull(orc_state_t *s, const trt_t *t)

@@ -66,6 +66,15 @@ int orc_run(int kernel, const int dims[3], const int periodic[3], const int *lat
             int iterations, int init_mode, const double *init_pdfs, double *out_pdfs,
             const int blk[3], int pad_mode);
 
+/* One half (odd = 0: even step, 1: odd step) of a list AA step pair over
+ * nodes [0, n_nodes) of f[d * n_cells + node] through the push adjacency adj
+ * (n_nodes * 18), with the per-step body force added at the access that
+ * follows each step; a complete pair equals orc_run's list AA pair bit for
+ * bit. For checking decomposed (slab) layouts whose ghost nodes follow the
+ * owned ones. */
+int orc_list_aa_half(int odd, int n_nodes, int n_cells, const uint32_t *adj, double *f,
+                     double omega, double lambda, double xforce);
+
 /* The reference's -verify check (src/Kernel.c:451-625) on a field of logical
  * PDFs (same layout as orc_run's out_pdfs). Returns the L2 norm of the
  * relative error of the x-velocity profile at x = nX/2. */

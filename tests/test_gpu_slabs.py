@@ -1,8 +1,9 @@
-"""One full-array AA lattice split into x-slabs (lbm_aa_slab_*, lbmb200.slabs):
-slabs in one process on one GPU, halo messages through device buffers on one
-stream, against the single-instance kernel -- bit for bit after every pair.
-(With one slab per GPU the messages travel through torch.distributed instead;
-that transport's pairing is tested on CPU ranks in test_slabs_gloo.py.)"""
+"""One AA-pattern lattice split into x-slabs (lbm_aa_slab_*, lbmb200.slabs),
+full-array (cuda-aa-soa) and list (cuda-list-aa-pv-soa) layouts: slabs in
+one process on one GPU, halo messages through device buffers on one stream,
+against the single-instance kernel -- bit for bit after every pair. (With one
+slab per GPU the messages travel through torch.distributed instead; that
+transport is tested on CPU ranks in test_slabs_gloo.py.)"""
 import numpy as np
 import pytest
 
@@ -27,13 +28,13 @@ CASES = [
 ]
 
 
-def _run_slabs(lat, parts, init, cd, pairs):
+def _run_slabs(lat, parts, init, cd, pairs, layout="full", kargs=("-lambda", "3/16")):
     import torch
     work = torch.cuda.Stream()  # an explicit stream orders all slabs' operations
     stream = work.cuda_stream
     ring = sl.is_ring(lat.periodic)
     ranges = sl.partition(lat.dims[0], parts)
-    slabs = [sl.Slab(lat, x0, x1, *sl.halo_flags(r, parts, ring), kernel_args=["-lambda", "3/16"])
+    slabs = [sl.Slab(lat, x0, x1, *sl.halo_flags(r, parts, ring), kernel_args=list(kargs), layout=layout)
              for r, (x0, x1) in enumerate(ranges)]
     try:
         sl.scatter_field(slabs, lat, init)
@@ -77,3 +78,68 @@ def test_slabrun_single_process(capsys):
     import json
     rec = json.loads(out)
     assert rec["ranks"] == 1 and rec["fluid_nodes"] == 32 * 16 * 16 and rec["mflups"] > 0
+
+
+LIST_CASES = CASES + [
+    ("spheres", (30, 24, 24), (1, 1, 1), 3),
+    ("spheres", (16, 16, 16), (1, 1, 1), 8),  # slabs of two planes
+]
+
+
+def _lattice(geo, dims, per):
+    if geo == "spheres":
+        return lbmb200.spheres(dims, 42, 0.45, 2.0, 4.0, 4000)[0]
+    return lbmb200.geometry(geo, dims, per)
+
+
+@pytest.mark.parametrize("geo,dims,per,parts", LIST_CASES)
+def test_list_slabs_equal_whole_lattice(geo, dims, per, parts):
+    lat = _lattice(geo, dims, per)
+    init = random_pdfs(lat.mask.size, 37)
+    cd = lbmb200.case(omega=1.1, xforce=2e-4, iterations=10)
+    kargs = ["-lambda", "3/16", "-pad", "no"]
+    inst = lbmb200.kernel("cuda-list-aa-pv-soa").init(lat, kernel_args=kargs)
+    try:
+        inst.set_field(init)
+        inst.run(cd)
+        whole = inst.get_field()
+    finally:
+        inst.deinit()
+    got = _run_slabs(lat, parts, init, cd, 5, layout="list", kargs=kargs)
+    m = lat.mask != 0
+    assert np.array_equal(got[m], whole[m])
+
+
+def test_list_slab_moments_sum_to_whole_lattice():
+    """FP64 conservation sums of the slabs' owned nodes add up to the whole
+    lattice's (the sums a multi-GPU run all-reduces)."""
+    lat = _lattice("spheres", (24, 20, 20), (1, 1, 1))
+    init = random_pdfs(lat.mask.size, 5)
+    inst = lbmb200.kernel("cuda-list-aa-pv-soa").init(lat, kernel_args=["-lambda", "3/16"])
+    try:
+        inst.set_field(init)
+        whole = np.array(inst.moments())
+    finally:
+        inst.deinit()
+    ring = sl.is_ring(lat.periodic)
+    slabs = [sl.Slab(lat, x0, x1, *sl.halo_flags(r, 3, ring), kernel_args=["-lambda", "3/16"], layout="list")
+             for r, (x0, x1) in enumerate(sl.partition(lat.dims[0], 3))]
+    try:
+        sl.scatter_field(slabs, lat, init)
+        parts = np.sum([np.array(s.inst.moments()) for s in slabs], axis=0)
+    finally:
+        for s in slabs:
+            s.close()
+    assert np.allclose(parts, whole, rtol=1e-12, atol=1e-12)
+
+
+def test_slabrun_list_layout_single_process(capsys):
+    from lbmb200 import slabrun
+    slabrun.main(["--dims", "32x24x24", "--geometry", "spheres:7:0.5:2:4", "--layout", "list",
+                  "--pairs", "2", "--warmup", "1"])
+    import json
+    rec = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert rec["layout"] == "list" and rec["mflups"] > 0
+    # the flow starts at rest with f = w: the mass is one per fluid node
+    assert abs(rec["sum_rho"] - rec["fluid_nodes"]) < 1e-9 * rec["fluid_nodes"]
+    assert rec["sum_jx"] > 0 and rec["permeability"] > 0

@@ -70,3 +70,72 @@ def test_dist_transport_pairs_faces(tmp_path, world, periodic):
                 assert rec["got"]["1/%d" % phase] == want
             else:
                 assert "1/%d" % phase not in rec["got"]
+
+
+LIST_SCRIPT = textwrap.dedent("""
+    import json, os, sys
+    sys.path[:0] = [os.path.join(%(root)r, "lbm-benchmark-kernels_b200"), os.path.join(%(root)r, "tests"),
+                    os.path.join(%(root)r, "oracle")]
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import lbmb200
+    from lbmb200.ranks import Ranks
+    from lbmb200 import slabs as sl
+    from oracle import Oracle
+    from slab_emu import EmuSlab, init_field
+
+    r = Ranks(backend="gloo", timeout_s=60)
+    geo, dims, per, pairs = sys.argv[1], tuple(int(v) for v in sys.argv[2].split("x")), \\
+        tuple(int(c) for c in sys.argv[3]), int(sys.argv[4])
+    lat = lbmb200.geometry(geo, dims, per)
+    ring = sl.is_ring(lat.periodic)
+    x0, x1 = sl.partition(dims[0], r.world)[r.rank]
+    lo, hi = sl.halo_flags(r.rank, r.world, ring)
+    slab = EmuSlab(lat, x0, x1, lo, hi, ("-pad", "no"))
+    slab.set_field(init_field(lat, 5))
+    tr = sl.DistTransport(slab, r.rank, r.world, ring, dist, lambda n: torch.zeros(n, dtype=torch.float64))
+    orc = Oracle()
+    for _ in range(pairs):
+        slab.half(orc, 0)
+        tr.exchange(0)
+        slab.half(orc, 1)
+        tr.exchange(1)
+    out = np.zeros((lat.mask.size, 19))
+    slab.get_field(out)
+    np.save(os.path.join(%(out)r, "part%%d.npy" %% r.rank), out[slab.gcells])
+    np.save(os.path.join(%(out)r, "cells%%d.npy" %% r.rank), slab.gcells)
+    r.close()
+""")
+
+
+@pytest.mark.parametrize("world,geo,dims,per", [(2, "fluid", "6x5x4", "111"), (3, "channel", "9x6x5", "110"),
+                                                 (2, "box", "8x5x5", "000")])
+def test_list_slabs_over_gloo_match_undivided_run(tmp_path, oracle, world, geo, dims, per):
+    """List-AA slabs as gloo ranks: the layout from the library, the steps
+    from the oracle, the halo messages through DistTransport; the gathered
+    field equals the undivided oracle run bit for bit."""
+    sys.path[:0] = [os.path.join(ROOT, "tests")]
+    import numpy as np
+    import lbmb200
+    from slab_emu import LAM, OMEGA, XF, init_field
+    script = tmp_path / "list_slab_probe.py"
+    script.write_text(LIST_SCRIPT % {"root": ROOT, "out": str(tmp_path)})
+    pairs = 3
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=%d" % world,
+           "--master-addr=127.0.0.1", "--master-port=%d" % (29571 + world + 7 * len(geo)), str(script),
+           geo, dims, per, str(pairs)]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=240, env=dict(os.environ, OMP_NUM_THREADS="1"))
+    assert out.returncode == 0, out.stderr[-3000:]
+    d = tuple(int(v) for v in dims.split("x"))
+    lat = lbmb200.geometry(geo, d, tuple(int(c) for c in per))
+    init = init_field(lat, 5)
+    want = oracle.run("list-aa", lat.dims, lat.periodic, lat.mask, omega=OMEGA, lam=LAM, xforce=XF,
+                      iterations=2 * pairs, init="pdfs", init_pdfs=init)
+    seen = 0
+    for rank in range(world):
+        cells = np.load(tmp_path / ("cells%d.npy" % rank))
+        part = np.load(tmp_path / ("part%d.npy" % rank))
+        assert np.array_equal(part, want[cells])
+        seen += cells.size
+    assert seen == lat.n_fluid
