@@ -166,6 +166,99 @@ long long list_build_device(const int* mask, const int dims[3], const int period
   return count;
 }
 
+// --- run-compressed adjacency ----------------------------------------------------
+
+// One block of kListTile threads per tile: the tile's head mask.
+__global__ void k_run_heads(const uint32_t* __restrict__ adj, int nFluid, uint32_t* __restrict__ mask) {
+  const long long n = (long long)blockIdx.x * kListTile + threadIdx.x;
+  bool head = false;
+  if (n < nFluid) {
+    head = threadIdx.x == 0;
+    for (int d = 0; d < QM && !head; ++d) head = adj[n * QM + d] != adj[(n - 1) * QM + d] + 1u;
+  }
+  const uint32_t m = __ballot_sync(0xffffffffu, head);
+  if ((threadIdx.x & 31) == 0) mask[(size_t)blockIdx.x * (kListTile / 32) + (threadIdx.x >> 5)] = m;
+}
+
+// Size of each tile's record in 16-byte units (entry nTiles: 0, so that the
+// exclusive sum ends with the total).
+__global__ void k_run_sizes(const uint32_t* __restrict__ mask, int nTiles, uint32_t* __restrict__ size16) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > nTiles) return;
+  if (t == nTiles) { size16[t] = 0; return; }
+  int h = 0;
+  for (int k = 0; k < kListTile / 32; ++k) h += __popc(mask[(size_t)t * (kListTile / 32) + k]);
+  const int h2 = (h + 1) & ~1;
+  size16[t] = (uint32_t)(kRunHdrWords / 4 + h2 * QM / 4);
+}
+
+__global__ void k_run_fill(const uint32_t* __restrict__ adj, int nFluid, const uint32_t* __restrict__ mask,
+                           const uint32_t* __restrict__ runOff, uint32_t* __restrict__ runs) {
+  const int t = blockIdx.x;
+  uint32_t* const rec = runs + (size_t)runOff[t] * 4;
+  const uint32_t* const m = mask + (size_t)t * (kListTile / 32);
+  if (threadIdx.x < kRunHdrWords) rec[threadIdx.x] = threadIdx.x < kListTile / 32 ? m[threadIdx.x] : 0u;
+  const long long n = (long long)t * kListTile + threadIdx.x;
+  if (n >= nFluid) return;
+  const int w = threadIdx.x >> 5, b = threadIdx.x & 31;
+  if (!((m[w] >> b) & 1u)) return;
+  int rank = 0;
+  for (int k = 0; k < w; ++k) rank += __popc(m[k]);
+  rank += __popc(m[w] & ((2u << b) - 1u)) - 1;  // heads before this one
+  uint32_t* const row = rec + kRunHdrWords + rank * QM;
+  for (int d = 0; d < QM; ++d) row[d] = adj[n * QM + d];
+}
+
+int list_runs_device(const uint32_t* adj, int nFluid, cudaStream_t s, uint32_t** runs, uint32_t** runOff,
+                     size_t* runBytes) {
+  *runs = nullptr;
+  *runOff = nullptr;
+  *runBytes = 0;
+  const int nTiles = (nFluid + kListTile - 1) / kListTile;
+  uint32_t *mask = nullptr, *size16 = nullptr;
+  void* tmp = nullptr;
+  size_t tmpBytes = 0;
+  uint32_t total = 0;
+  cudaError_t e = cudaMalloc(runOff, sizeof(uint32_t) * (nTiles + 1));
+  if (e == cudaSuccess) e = cudaMallocAsync(&mask, sizeof(uint32_t) * (size_t)(nTiles > 0 ? nTiles : 1) * 8, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&size16, sizeof(uint32_t) * (nTiles + 1), s);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tmpBytes, size16, *runOff, nTiles + 1, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&tmp, tmpBytes, s);
+  if (e == cudaSuccess && nTiles > 0) {
+    k_run_heads<<<nTiles, kListTile, 0, s>>>(adj, nFluid, mask);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    k_run_sizes<<<(nTiles + 1 + 255) / 256, 256, 0, s>>>(mask, nTiles, size16);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tmpBytes, size16, *runOff, nTiles + 1, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&total, *runOff + nTiles, 4, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) {
+    *runBytes = (size_t)(total > 0 ? total : 1) * 16;
+    e = cudaMalloc(runs, *runBytes);
+  }
+  if (e == cudaSuccess) e = cudaMemsetAsync(*runs, 0, *runBytes, s);
+  if (e == cudaSuccess && nTiles > 0) {
+    k_run_fill<<<nTiles, kListTile, 0, s>>>(adj, nFluid, mask, *runOff, *runs);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFreeAsync(tmp, s);
+  cudaFreeAsync(size16, s);
+  cudaFreeAsync(mask, s);
+  cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    cudaFree(*runs);
+    cudaFree(*runOff);
+    *runs = nullptr;
+    *runOff = nullptr;
+    return (int)e;
+  }
+  return 0;
+}
+
 }  // namespace lbm
 
 extern "C" {

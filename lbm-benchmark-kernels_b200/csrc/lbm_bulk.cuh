@@ -6,6 +6,8 @@
 #pragma once
 #include <cstdint>
 
+#include "lbm_kernels.cuh"
+
 namespace lbm {
 
 constexpr uint32_t kBulkSpinLimit = 1u << 22;  // try_wait rounds before giving up
@@ -53,6 +55,56 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   for (uint32_t i = 0; i < kBulkSpinLimit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
+}
+
+// Stages the run record of tile blockIdx.x (run-compressed adjacency, see
+// kRunHdrWords) into srun (kRunTileWords words) with one bulk copy. A record
+// whose size does not fit flags error bit 4 and is not copied. After the
+// wait, warp 1 prefetches into L2 the record of the tile `a.prefetch` tiles
+// ahead (the block that will take this one's place), off the block's
+// critical path. Returns false (error word set) if the copy did not arrive
+// within the spin limit or was refused; every thread returns the same.
+template <class A>
+__device__ __forceinline__ bool stage_run_tile(const A& a, uint32_t* srun, uint64_t* bar, int* ok) {
+  if (threadIdx.x == 0) {
+    const uint32_t o0 = a.runOff[blockIdx.x], o1 = a.runOff[blockIdx.x + 1];
+    const uint32_t bytes = (o1 - o0) * 16u;
+    *ok = o1 > o0 && bytes <= static_cast<uint32_t>(kRunTileWords) * 4u;
+    mbar_init(bar, 1);
+    if (*ok) {
+      mbar_arrive_expect_tx(bar, bytes);
+      bulk_g2s(srun, a.runs + static_cast<size_t>(o0) * 4, bytes, bar);
+    } else {
+      atomicOr(a.err, 4);
+    }
+  }
+  __syncthreads();
+  if (!*ok) return false;
+  if (!mbar_wait_bounded(bar, 0)) {
+    if (threadIdx.x == 0) atomicOr(a.err, 1);
+    return false;
+  }
+  if (threadIdx.x == 32 && a.prefetch > 0 && blockIdx.x + static_cast<unsigned>(a.prefetch) < gridDim.x) {
+    const unsigned t = blockIdx.x + a.prefetch;
+    const uint32_t o0 = a.runOff[t], o1 = a.runOff[t + 1];
+    if (o1 > o0 && (o1 - o0) * 16u <= static_cast<uint32_t>(kRunTileWords) * 4u)
+      bulk_prefetch_l2(a.runs + static_cast<size_t>(o0) * 4, (o1 - o0) * 16u);
+  }
+  return true;
+}
+
+// The adjacency row of node `tid` of a staged run record and the node's
+// distance from its run's head: link d of the node is row[d] + off.
+__device__ __forceinline__ const uint32_t* run_row(const uint32_t* srun, int tid, uint32_t& off) {
+  const int w = tid >> 5, b = tid & 31;
+  int rank = 0;
+  for (int k = 0; k < w; ++k) rank += __popc(srun[k]);
+  uint32_t mk = srun[w] & ((2u << b) - 1u);
+  rank += __popc(mk);
+  int k = w;
+  while (mk == 0u && k > 0) mk = srun[--k];  // node 0 of a tile always heads a run
+  off = mk ? static_cast<uint32_t>(tid - (32 * k + 31 - __clz(mk))) : 0u;
+  return srun + kRunHdrWords + (rank > 0 ? rank - 1 : 0) * 18;
 }
 
 }  // namespace lbm

@@ -83,6 +83,9 @@ struct Gpu {
   // list layout
   uint32_t* grid;
   uint32_t* adjHost;
+  uint32_t* dRuns;    // run-compressed adjacency (list AA and list push kernels)
+  uint32_t* dRunOff;
+  size_t runBytes;
   int nFluid, nCells;
   int cur;  // pull: index of the current grid (0 = dF, 1 = dG)
 
@@ -313,6 +316,8 @@ lbm::ListArgs list_args(Gpu* g) {
   a.f = g->cur == 0 ? g->dF : g->dG;
   a.g = g->cur == 0 ? g->dG : g->dF;
   a.adj = g->dAdj;
+  a.runs = g->dRuns;
+  a.runOff = g->dRunOff;
   a.nCells = g->nCells;
   a.nFluid = g->nFluid;
   a.err = g->dErr;
@@ -324,6 +329,8 @@ lbm::ListArgsLp list_args_lp(Gpu* g) {
   a.prefetch = list_prefetch_enabled();
   a.f = g->dF;
   a.adj = g->dAdj;
+  a.runs = g->dRuns;
+  a.runOff = g->dRunOff;
   a.nCells = g->nCells;
   a.nFluid = g->nFluid;
   a.err = g->dErr;
@@ -707,6 +714,14 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* sla
     }
     LBM_CK(cudaFree(dGrid));
     LBM_CK(cudaFree(dMask));
+    if (kind == kListAa || kind == kListPush) {
+      // the odd step (list AA) and the push step read the run-compressed form
+      const int rc = lbm::list_runs_device(g->dAdj, g->nFluid, g->stream, &g->dRuns, &g->dRunOff, &g->runBytes);
+      if (rc) {
+        std::printf("ERROR: CUDA: run-compressed adjacency: %s\n", cudaGetErrorString((cudaError_t)rc));
+        std::exit(1);
+      }
+    }
     g->mirrorElems = (size_t)Q * nCells;
     LBM_CK(cudaMalloc(&g->dF, g->elemBytes * g->mirrorElems));
     LBM_CK(cudaMemset(g->dF, 0, g->elemBytes * g->mirrorElems));
@@ -747,6 +762,8 @@ void gpu_free(KernelData** kernelData) {
   cudaFree(g->dOddBlocks);
   std::free(g->sliceMask);
   cudaFree(g->dAdj);
+  cudaFree(g->dRuns);
+  cudaFree(g->dRunOff);
   for (int side = 0; side < 2; ++side)
     for (int list = 0; list < 2; ++list) cudaFree(g->dHalo[side][list]);
   cudaFree(g->dErr);

@@ -68,6 +68,18 @@ void aa_halo_unpack(const AaArgs& a, int side, int phase, const double* buf, cud
 // tile can be fetched with one bulk copy.
 constexpr int kListTile = 256;
 
+// Run-compressed adjacency (the reference's consecutive nodes,
+// src/BenchKernelD3Q19ListAaPvCommon.c:326-469, cut at tiles of kListTile
+// nodes): node n starts a run unless every link of n is the same link of
+// n - 1 plus one, and a tile's first node always starts one. Per tile, at
+// runs + 4 * runOff[t] (16-byte units): a header of kRunHdrWords words (the
+// head mask: bit k of word w = node 32 w + k of the tile starts a run; 4
+// zero words) and one 18-entry row per head, the head count rounded up to
+// even (a multiple of 16 bytes). A node's link d is its head's link d plus
+// its distance from the head.
+constexpr int kRunHdrWords = 12;
+constexpr int kRunTileWords = kRunHdrWords + kListTile * 18;
+
 struct ListArgs {
   double* f;      // list AA: the one grid; pull: source grid
   double* g;      // pull: destination grid
@@ -76,6 +88,8 @@ struct ListArgs {
   int nFluid;
   int* err;       // device error word (bounded waits)
   int prefetch;   // tiles ahead whose adjacency a block prefetches into L2 (0: none)
+  const uint32_t* runs;    // run-compressed adjacency (list AA odd step, list push)
+  const uint32_t* runOff;  // nTiles + 1 tile offsets into runs, 16-byte units
 };
 
 // The prefetch distance of a launch of `kernel` (threads per block): its
@@ -111,6 +125,8 @@ constexpr int kLpTileNodes = 1024;
 struct ListArgsLp {
   void* f;  // float or __half, f[d * nCells + n]
   const uint32_t* adj;
+  const uint32_t* runs;    // as ListArgs
+  const uint32_t* runOff;
   long long nCells;
   int nFluid;
   int* err;
@@ -128,6 +144,13 @@ long long list_build_device(const int* mask, const int dims[3], const int period
 // f[idx[k]] = buf[k] (scatter) for k < n.
 void slot_gather(const double* f, const uint32_t* idx, long long n, double* buf, cudaStream_t s);
 void slot_scatter(double* f, const uint32_t* idx, long long n, const double* buf, cudaStream_t s);
+
+// Run-compressed adjacency of the nFluid nodes of adj (device, 18 entries
+// per node): allocates *runs (cudaMalloc, *runBytes bytes) and *runOff
+// (nTiles + 1 entries) and fills them; synchronises s. Returns 0 or a CUDA
+// error code.
+int list_runs_device(const uint32_t* adj, int nFluid, cudaStream_t s, uint32_t** runs, uint32_t** runOff,
+                     size_t* runBytes);
 
 // Launchers (stream-ordered, no synchronisation).
 void list_even_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s);

@@ -113,41 +113,28 @@ __global__ void __launch_bounds__(256) k_list_even_staged(const ListArgsLp a, co
   }
 }
 
-__device__ __forceinline__ bool stage_adj_tile_lp(const ListArgsLp& a, uint32_t* sadj, uint64_t* bar) {
-  if (threadIdx.x == 0) {
-    mbar_init(bar, 1);
-    mbar_arrive_expect_tx(bar, kListTile * QM * 4);
-    bulk_g2s(sadj, a.adj + static_cast<size_t>(blockIdx.x) * kListTile * QM, kListTile * QM * 4, bar);
-    const unsigned ahead = blockIdx.x + a.prefetch;
-    if (a.prefetch > 0 && ahead < gridDim.x)
-      bulk_prefetch_l2(a.adj + static_cast<size_t>(ahead) * kListTile * QM, kListTile * QM * 4);
-  }
-  __syncthreads();
-  if (!mbar_wait_bounded(bar, 0)) {
-    if (threadIdx.x == 0) atomicOr(a.err, 1);
-    return false;
-  }
-  return true;
-}
-
 template <class St>
 __global__ void __launch_bounds__(kListTile) k_list_odd_lp(const ListArgsLp a, const Trt<float> t) {
   using T = typename St::T;
-  __shared__ alignas(128) uint32_t sadj[kListTile * QM];
+  __shared__ alignas(128) uint32_t srun[kRunTileWords];
   __shared__ alignas(8) uint64_t bar;
-  if (!stage_adj_tile_lp(a, sadj, &bar)) return;
+  __shared__ int ok;
+  if (!stage_run_tile(a, srun, &bar, &ok)) return;
   const int n = blockIdx.x * kListTile + threadIdx.x;
   if (n >= a.nFluid) return;
-  const uint32_t* e = sadj + threadIdx.x * QM;
+  uint32_t off;
+  const uint32_t* e = run_row(srun, threadIdx.x, off);  // link d = e[d] + off (run-compressed adjacency)
   T* const f = static_cast<T*>(a.f);
   const long long S = a.nCells;
-  auto load = [&](int d) -> float { return St::dev(d == DC ? f[DC * S + n] : f[e[inv(d)]], d) + t.force[d]; };
+  auto load = [&](int d) -> float {
+    return St::dev(d == DC ? f[DC * S + n] : f[e[inv(d)] + off], d) + t.force[d];
+  };
   auto store = [&](int d, float v) {
     if (d == DC) {
       f[DC * S + n] = St::raw(v + t.force[DC], DC);
       return;
     }
-    const uint32_t dst = reinterpret_cast<const volatile uint32_t*>(e)[d];  // re-read: keeps no 64-bit addresses live across the collision
+    const uint32_t dst = reinterpret_cast<const volatile uint32_t*>(e)[d] + off;  // re-read: keeps no 64-bit addresses live across the collision
     const int j = inv(d);
     const bool bounce = dst == static_cast<uint32_t>(j * S + n);
     f[dst] = St::raw(v + (bounce ? t.force[j] : t.force[d]), d);  // the scale is equal for d and inv(d)
