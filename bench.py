@@ -40,7 +40,15 @@ PKG = os.path.join(ROOT, "lbm-benchmark-kernels_b200")
 sys.path.insert(0, PKG)
 
 L2_BYTES = 126 * 1024 * 1024
-B_PER_FLUP = {"even": 2 * 19 * 8, "odd": 2 * 19 * 8 + 18 * 4, "pull": 2 * 19 * 8 + 18 * 4, "aa": 2 * 19 * 8}
+B_PER_FLUP = {"even": 2 * 19 * 8, "aa": 2 * 19 * 8}
+
+
+def adjacency_bytes_per_node(lbmb200, inst, n_fluid):
+    """Adjacency bytes per node that one adjacency-driven launch reads (run
+    records for the list AA odd and list push steps, whole tiles for pull)."""
+    L = lbmb200.lib()
+    L.lbm_b200_adjacency_bytes.restype = ctypes.c_longlong
+    return L.lbm_b200_adjacency_bytes(inst.kdp) / max(1, n_fluid)
 
 
 def parse():
@@ -438,6 +446,8 @@ def run_ours(args, dist):
     clocks.start()
     t = time_kernel(lbmb200, "cuda-list-aa-pv-soa", lat, args.steps, max(3, args.warmup), kargs, dist, "odd")
     inst = t["inst"]
+    adj_node = adjacency_bytes_per_node(lbmb200, inst, lat.n_fluid)
+    odd_bpf = B_PER_FLUP["even"] + adj_node
     try:
         # e2e: the reference-facing Kernel() call, mirror uploaded and downloaded
         cd = lbmb200.case(omega=1.0, xforce=1e-5, iterations=500)
@@ -463,7 +473,7 @@ def run_ours(args, dist):
     odd = per[1::2]
     odd_ms = statistics.mean(odd)
     even_ms = statistics.mean(even)
-    achieved = B_PER_FLUP["odd"] * lat.n_fluid / (odd_ms / 1e3) / 1e9
+    achieved = odd_bpf * lat.n_fluid / (odd_ms / 1e3) / 1e9
     traffic = profile_traffic("list_odd_fp64")
     line = {
         "metric": "MFLUP/s & % HBM roofline at 256^3", "value": round(value, 3), "unit": "MFLUP/s",
@@ -474,7 +484,9 @@ def run_ours(args, dist):
         "roofline": {"bound": "hbm", "kernel": "k_list_odd_fp64 (adjacency-driven odd step)",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                     "bytes_per_flup": B_PER_FLUP["odd"], "launch_ms": round(odd_ms, 5),
+                     "bytes_per_flup": round(odd_bpf, 2),
+                     "adjacency": "run-compressed: %.2f B per node (72 uncompressed)" % adj_node,
+                     "launch_ms": round(odd_ms, 5),
                      "traffic": traffic,
                      "even_step": {"bytes_per_flup": B_PER_FLUP["even"], "launch_ms": round(even_ms, 5),
                                    "achieved": round(B_PER_FLUP["even"] * lat.n_fluid / (even_ms / 1e3) / 1e9, 1)}},
@@ -489,20 +501,24 @@ def run_ours(args, dist):
         extra = {}
         # pull kernel on the same domain
         tp = time_kernel(lbmb200, "cuda-list-pull-split-nt-1s-soa", lat, min(args.steps, 200), 3, kargs, dist, "pull")
+        bpf = B_PER_FLUP["even"] + adjacency_bytes_per_node(lbmb200, tp["inst"], lat.n_fluid)
         tp["inst"].deinit()
         pm = statistics.mean(tp["per_launch_ms"])
         extra["cuda-list-pull-split-nt-1s-soa"] = {
             "mflups": round(lat.n_fluid / (pm / 1e3) / 1e6, 1), "launch_ms": round(pm, 5),
-            "achieved_gbs": round(B_PER_FLUP["pull"] * lat.n_fluid / (pm / 1e3) / 1e9, 1),
-            "frac": round(B_PER_FLUP["pull"] * lat.n_fluid / (pm / 1e3) / 1e9 / peak, 4)}
-        # the two-grid list rows on the same domain (376 B per node update)
+            "bytes_per_flup": round(bpf, 2),
+            "achieved_gbs": round(bpf * lat.n_fluid / (pm / 1e3) / 1e9, 1),
+            "frac": round(bpf * lat.n_fluid / (pm / 1e3) / 1e9 / peak, 4)}
+        # the two-grid list rows on the same domain (304 B of PDFs plus the adjacency each reads per node update)
         for kname in ("cuda-list-push-soa", "cuda-list-pull-soa"):
             tq = time_kernel(lbmb200, kname, lat, min(args.steps, 200), 3, kargs, dist, "pull")
+            bpf = B_PER_FLUP["even"] + adjacency_bytes_per_node(lbmb200, tq["inst"], lat.n_fluid)
             tq["inst"].deinit()
             qm = statistics.mean(tq["per_launch_ms"])
             extra[kname] = {"mflups": round(lat.n_fluid / (qm / 1e3) / 1e6, 1), "launch_ms": round(qm, 5),
-                            "achieved_gbs": round(B_PER_FLUP["pull"] * lat.n_fluid / (qm / 1e3) / 1e9, 1),
-                            "frac": round(B_PER_FLUP["pull"] * lat.n_fluid / (qm / 1e3) / 1e9 / peak, 4)}
+                            "bytes_per_flup": round(bpf, 2),
+                            "achieved_gbs": round(bpf * lat.n_fluid / (qm / 1e3) / 1e9, 1),
+                            "frac": round(bpf * lat.n_fluid / (qm / 1e3) / 1e9 / peak, 4)}
         # full-array AA at 256^3: the reference's -geometry fluid with -periodic-x -periodic-y
         # -periodic-z, and -geometry channel (x periodic, walls in y and z)
         for key, geo, per_flags in (("cuda-aa-soa", "fluid", (1, 1, 1)), ("cuda-aa-soa/channel", "channel", (0, 0, 0))):
@@ -524,11 +540,12 @@ def run_ours(args, dist):
         for prec, pb in (("fp32", 4), ("fp16", 2)):
             tl = time_kernel(lbmb200, "cuda-list-aa-pv-soa", lat, min(args.steps, 200), 4,
                              kargs + ["-precision", prec], dist, "odd")
+            # mean of the even (38 s) and odd (38 s + adjacency) steps
+            bpf = 2 * 19 * pb + adjacency_bytes_per_node(lbmb200, tl["inst"], lat.n_fluid) / 2
             tl["inst"].deinit()
             m = statistics.mean(tl["per_launch_ms"])
-            bpf = 2 * 19 * pb + 36
             extra["cuda-list-aa-pv-soa/" + prec] = {
-                "mflups": round(lat.n_fluid / (m / 1e3) / 1e6, 1), "bytes_per_flup": bpf,
+                "mflups": round(lat.n_fluid / (m / 1e3) / 1e6, 1), "bytes_per_flup": round(bpf, 2),
                 "achieved_gbs": round(bpf * lat.n_fluid / (m / 1e3) / 1e9, 1),
                 "frac": round(bpf * lat.n_fluid / (m / 1e3) / 1e9 / peak, 4),
                 "even_ms": round(statistics.mean(tl["per_launch_ms"][0::2]), 5),

@@ -252,6 +252,13 @@ int lbm_b200_time_steps(KernelData *kd, CaseData *cd, int n, double *total_ms, d
  * reversed links; face shell), list AA 2 per pair, pull 1 per step. */
 long lbm_b200_launches_for(KernelData *kd, int n);
 
+/* Adjacency bytes one adjacency-driven launch of a list instance reads (the
+ * list AA odd step, the push and the pull steps): the run-compressed
+ * records -- one 18-entry row per run of consecutive nodes whose links all
+ * advance by one (the reference's consecutive nodes, cut at 256-node tiles)
+ * plus a 48-byte header per tile. 0 for the full-array kernels. */
+long long lbm_b200_adjacency_bytes(KernelData *kd);
+
 /* ---- x-slabs of an AA-pattern lattice (one lattice over several GPUs) ----
  * No counterpart in the reference, whose kernels address one array; the
  * slabs reproduce the undivided lattice's run bit for bit.

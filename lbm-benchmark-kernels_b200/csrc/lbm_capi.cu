@@ -714,8 +714,9 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* sla
     }
     LBM_CK(cudaFree(dGrid));
     LBM_CK(cudaFree(dMask));
-    if (kind == kListAa || kind == kListPush) {
-      // the odd step (list AA) and the push step read the run-compressed form
+    {
+      // the adjacency-driven steps read the run-compressed form (the full
+      // adjacency stays for the host layout queries)
       const int rc = lbm::list_runs_device(g->dAdj, g->nFluid, g->stream, &g->dRuns, &g->dRunOff, &g->runBytes);
       if (rc) {
         std::printf("ERROR: CUDA: run-compressed adjacency: %s\n", cudaGetErrorString((cudaError_t)rc));
@@ -732,9 +733,11 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* sla
     kd->GlobalDims[0] = ld->Dims[0];
     kd->GlobalDims[1] = ld->Dims[1];
     kd->GlobalDims[2] = ld->Dims[2];
-    // the GPU odd step reads all 18 adjacency entries of a node every time
+    // bytes per node update: the PDFs plus the adjacency the step reads
+    // (run-compressed for the list AA odd and list push steps)
     const double pb = 2.0 * 19 * (double)g->elemBytes;
-    kd->LoopBalance = two_grid(kind) ? pb + 18 * 4.0 : (pb + (pb + 18 * 4.0)) / 2.0;
+    const double ab = g->dRuns && g->nFluid > 0 ? (double)g->runBytes / g->nFluid : 18 * 4.0;
+    kd->LoopBalance = two_grid(kind) ? pb + ab : (pb + (pb + ab)) / 2.0;
   }
 
   LBM_CK(cudaMallocHost(&g->mirror, sizeof(double) * g->mirrorElems));
@@ -951,6 +954,12 @@ int lbm_b200_sync_mirror(KernelData* kd) {
 const char* lbm_b200_last_error(void) { return g_lastError.c_str(); }
 
 long lbm_b200_launches_for(KernelData* kd, int n) { return launches_for(reinterpret_cast<Gpu*>(kd), n); }
+
+long long lbm_b200_adjacency_bytes(KernelData* kd) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (full_array(g->kind)) return 0;
+  return (long long)g->runBytes;
+}
 
 // --- x-slabs of an AA-pattern lattice (full-array and list layouts) -------------
 

@@ -454,23 +454,6 @@ __global__ void __launch_bounds__(kListTile, 4) k_list_even_fp64(const ListArgs 
   trt_update(t, [&](int d) { return f[d * S]; }, [&](int d, double v) { fs[inv(d) * S] = v; });
 }
 
-// Stages the block's adjacency tile (kListTile nodes x 18 entries, contiguous)
-// into shared memory with one bulk copy. Returns false (and flags the error
-// word) if the copy does not complete within the spin limit.
-__device__ __forceinline__ bool stage_adj_tile(const ListArgs& a, uint32_t* sadj, uint64_t* bar) {
-  if (threadIdx.x == 0) {
-    mbar_init(bar, 1);
-    mbar_arrive_expect_tx(bar, kListTile * QM * 4);
-    bulk_g2s(sadj, a.adj + static_cast<size_t>(blockIdx.x) * kListTile * QM, kListTile * QM * 4, bar);
-  }
-  __syncthreads();
-  if (!mbar_wait_bounded(bar, 0)) {
-    if (threadIdx.x == 0) atomicOr(a.err, 1);
-    return false;
-  }
-  return true;
-}
-
 // 3 blocks of 256 threads per SM. The adjacency comes run-compressed (one
 // row per run of consecutive nodes, see kRunHdrWords): at the 256^3 sphere
 // packing 0.49 rows per node, 35 instead of 72 bytes per node.
@@ -505,19 +488,21 @@ __global__ void __launch_bounds__(kListTile, 3) k_list_odd_fp64(const ListArgs a
 }
 
 __global__ void __launch_bounds__(kListTile) k_list_pull_fp64(const ListArgs a, const Trt<double> t) {
-  __shared__ alignas(128) uint32_t sadj[kListTile * QM];
+  __shared__ alignas(128) uint32_t srun[kRunTileWords];
   __shared__ alignas(8) uint64_t bar;
-  if (!stage_adj_tile(a, sadj, &bar)) return;
+  __shared__ int ok;
+  if (!stage_run_tile(a, srun, &bar, &ok)) return;
   const int n = blockIdx.x * kListTile + threadIdx.x;
   if (n >= a.nFluid) return;
-  const uint32_t* e = sadj + threadIdx.x * QM;
+  uint32_t off;
+  const uint32_t* e = run_row(srun, threadIdx.x, off);  // link d = e[d] + off (run-compressed pull adjacency)
   const long long S = a.nCells;
   // one pass: the gathers are issued together and the 19 outputs are
   // contiguous stores to the second grid
   double f[Q], o[Q];
   f[DC] = a.f[DC * S + n];
 #pragma unroll
-  for (int d = 0; d < QM; ++d) f[d] = a.f[e[d]];
+  for (int d = 0; d < QM; ++d) f[d] = a.f[e[d] + off];
   trt_collide(t, f, o);
 #pragma unroll
   for (int d = 0; d < Q; ++d) a.g[d * S + n] = o[d] + t.force[d];
@@ -583,8 +568,8 @@ void list_odd_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s) {
   k_list_odd_fp64<<<list_blocks(b), kListTile, 0, s>>>(b, t);
 }
 void list_pull_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s) {
-  // no adjacency prefetch: the pull step already runs at the copy bandwidth,
-  // and prefetching slowed it by 8 % on a 256^3 sphere packing
+  // no adjacency prefetch: with the full adjacency it slowed this kernel by
+  // 8 % on a 256^3 sphere packing
   if (a.nFluid <= 0) return;
   ListArgs b = a;
   b.prefetch = 0;
