@@ -42,7 +42,8 @@ struct DomainSlot {
   bool active = false;
   lbm::BatchDomain dev{};  // as uploaded to the device table
   void* pdfs = nullptr;
-  uint32_t* adj = nullptr;
+  uint32_t* runs = nullptr;    // run-compressed adjacency
+  uint32_t* runOff = nullptr;
   int nTiles = 0;
   size_t bytes = 0;
   int dims[3] = {0, 0, 0};
@@ -157,8 +158,12 @@ int enqueue(Batch* b, int nsteps) {
   return 0;
 }
 
+// Bound on a domain's device bytes: PDFs plus the adjacency (full rows
+// while the run-compressed form is built from them; the runs never exceed
+// the full rows plus a 48-byte header per tile).
 size_t domain_bytes(const Batch* b, long long nCells) {
-  return (size_t)nCells * Q * b->elemBytes + (size_t)nCells * QM * 4;
+  return (size_t)nCells * Q * b->elemBytes + (size_t)nCells * QM * 4 +
+         (size_t)(nCells / lbm::kBatchTileNodes) * lbm::kRunHdrWords * 4;
 }
 
 lbm::TrtW trt_of(double omega, double lambda, double xforce) {
@@ -254,7 +259,8 @@ void lbm_batch_destroy(void* h) {
   drop_graphs(b);
   for (auto& s : b->slots) {
     cudaFree(s.pdfs);
-    cudaFree(s.adj);
+    cudaFree(s.runs);
+    cudaFree(s.runOff);
   }
   cudaFree(b->dDoms);
   cudaFree(b->dTileDom);
@@ -291,9 +297,11 @@ int lbm_batch_add(void* h, const LatticeDesc* ld, double omega, double lambda, d
   const long ncell = (long)ld->Dims[0] * ld->Dims[1] * ld->Dims[2];
   d.grid.resize(ncell);
   BCK(cudaMalloc(&d.pdfs, (size_t)nCells * Q * b->elemBytes));
-  BCK(cudaMalloc(&d.adj, (size_t)nCells * QM * 4));
+  uint32_t* adj = nullptr;
+  BCK(cudaMalloc(&adj, (size_t)nCells * QM * 4));
   // numbering and adjacency built on the device (lbm_build.cu); padding
-  // nodes then point at their own slots so that every entry is in range
+  // nodes then point at their own slots so that every entry is in range;
+  // the steps read the run-compressed form, built from it
   int* dMask = nullptr;
   uint32_t* dGrid = nullptr;
   BCK(cudaMallocAsync(&dMask, sizeof(int) * ncell, b->stream));
@@ -301,19 +309,23 @@ int lbm_batch_add(void* h, const LatticeDesc* ld, double omega, double lambda, d
   BCK(cudaMemcpyAsync(dMask, ld->Lattice, sizeof(int) * ncell, cudaMemcpyHostToDevice, b->stream));
   const int blk[3] = {0, 0, 0}, per[3] = {ld->PeriodicX, ld->PeriodicY, ld->PeriodicZ};
   const char* berr = "";
-  const long long nf = lbm::list_build_device(dMask, ld->Dims, per, 0, blk, (int)nCells, dGrid, d.adj, nCells,
+  const long long nf = lbm::list_build_device(dMask, ld->Dims, per, 0, blk, (int)nCells, dGrid, adj, nCells,
                                               b->stream, &berr);
   if (nf == nFluid) {
-    lbm::batch_pad_adjacency(d.adj, nFluid, nCells, b->stream);
+    lbm::batch_pad_adjacency(adj, nFluid, nCells, b->stream);
     BCK(cudaMemcpyAsync(d.grid.data(), dGrid, sizeof(uint32_t) * ncell, cudaMemcpyDeviceToHost, b->stream));
   }
   cudaFreeAsync(dGrid, b->stream);
   cudaFreeAsync(dMask, b->stream);
   BCK(cudaStreamSynchronize(b->stream));
-  if (nf != nFluid) {
-    g_batchError = nf < 0 ? berr : "the mask's fluid cell count differs from the lattice's";
+  int rrc = 0;
+  size_t runBytes = 0;
+  if (nf == nFluid) rrc = lbm::list_runs_device(adj, (int)nCells, b->stream, &d.runs, &d.runOff, &runBytes);
+  cudaFree(adj);
+  if (nf != nFluid || rrc) {
+    g_batchError = rrc ? "building the run-compressed adjacency failed"
+                       : (nf < 0 ? berr : "the mask's fluid cell count differs from the lattice's");
     cudaFree(d.pdfs);
-    cudaFree(d.adj);
     d = DomainSlot();
     return -6;
   }
@@ -325,7 +337,8 @@ int lbm_batch_add(void* h, const LatticeDesc* ld, double omega, double lambda, d
   d.lambda = lambda;
   d.xforce = xforce;
   d.dev.f = d.pdfs;
-  d.dev.adj = d.adj;
+  d.dev.runs = d.runs;
+  d.dev.runOff = d.runOff;
   d.dev.nCells = nCells;
   d.dev.nFluid = nFluid;
   d.dev.trt = trt_of(omega, lambda, xforce);
@@ -342,7 +355,8 @@ int lbm_batch_remove(void* h, int slot) {
   BCK(cudaStreamSynchronize(b->stream));
   DomainSlot& d = b->slots[slot];
   cudaFree(d.pdfs);
-  cudaFree(d.adj);
+  cudaFree(d.runs);
+  cudaFree(d.runOff);
   b->used -= d.bytes;
   d = DomainSlot();
   return publish(b);

@@ -20,7 +20,8 @@ constexpr int kBatchTileNodes = 256;  // node granularity of a domain's tiles
 
 struct BatchDomain {
   void* f;                // PDFs, storage format of the batch, f[d * nCells + n]
-  const uint32_t* adj;    // nTiles * kBatchTileNodes * 18 entries
+  const uint32_t* runs;   // run-compressed adjacency of the nCells nodes (kRunHdrWords)
+  const uint32_t* runOff; // nTiles + 1 record offsets, 16-byte units
   long long nCells;       // padded node count (a multiple of kBatchTileNodes)
   int nFluid;
   int tileStart;          // first tile of this domain in the tile table
@@ -32,11 +33,12 @@ struct BatchDomain {
 // per tile, from an address that depends on the tile index alone, so the
 // record of a block's next tile is fetched while the current one is updated.
 struct BatchTile {
-  const uint32_t* adj;  // this tile's adjacency block, kBatchTileNodes x 18 entries
+  const uint32_t* run;  // this tile's run record (run-compressed adjacency)
   void* f;              // the domain's PDFs
   int nCells;           // PDF plane stride of the domain (nCells * 19 < 2^32)
   int n0;               // domain-local index of the tile's first node
   int nValid;           // fluid nodes in the tile (0..kBatchTileNodes)
+  uint32_t runBytes;    // size of the run record (a multiple of 16)
   TrtW trt;             // relaxation rates and body force of the domain
 };
 constexpr int kTileWords = static_cast<int>(sizeof(BatchTile) / 4);  // one word per lane of a warp
@@ -62,7 +64,8 @@ struct BatchLaunch {
 
 // Adjacency rows of the padding nodes [nFluid, nCells): each entry points at
 // the node's own slot of the inverse direction (always in range, never read
-// back into a fluid node).
+// back into a fluid node). Padding rows advance by one from node to node, so
+// a tile's padding is one run in the run-compressed form.
 void batch_pad_adjacency(uint32_t* adj, int nFluid, long long nCells, cudaStream_t s);
 
 // Builds the tile records of tiles [0, nTiles).

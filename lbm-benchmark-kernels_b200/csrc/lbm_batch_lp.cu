@@ -2,10 +2,11 @@
 // (FP32 arithmetic on FP32 or FP16-deviation storage, as lbm_kernels_lp.cu).
 //
 // Every block walks the tile records with a grid stride (one tile per block
-// when the grid covers the table). The odd step stages a tile's adjacency
-// (256 nodes x 18 entries, 18 KB, contiguous) into shared memory with one
-// bulk copy, double buffered: while a tile is relaxed, the bulk copy of the
-// block's next tile is already in flight.
+// when the grid covers the table). The odd step stages a tile's run record
+// (run-compressed adjacency of 256 nodes, at most 18480 bytes, contiguous)
+// into shared memory with one bulk copy, double buffered in the persistent
+// kernel: while a tile is relaxed, the bulk copy of the block's next tile is
+// already in flight.
 #include "lbm_batch.cuh"
 #include "lbm_bulk.cuh"
 #include "lbm_store.cuh"
@@ -65,19 +66,26 @@ __global__ void __launch_bounds__(256) k_batch_even(const BatchArgs a) {
   }
 }
 
+// One node of a tile whose run record is staged in srun (local = the node's
+// index in the tile): link d is e[d] + off.
 template <class St>
-__device__ __forceinline__ void batch_odd_node(const BatchTile& T, const uint32_t* e, int n) {
+__device__ __forceinline__ void batch_odd_node(const BatchTile& T, const uint32_t* srun, int local) {
   using T_ = typename St::T;
+  uint32_t off;
+  const uint32_t* e = run_row(srun, local, off);
+  const int n = T.n0 + local;
   T_* const f = static_cast<T_*>(T.f);
   const long long S = T.nCells;
   const TrtW& t = T.trt;
-  auto load = [&](int d) -> float { return St::dev(d == DC ? f[DC * S + n] : f[e[inv(d)]], d) + t.force(d); };
+  auto load = [&](int d) -> float {
+    return St::dev(d == DC ? f[DC * S + n] : f[e[inv(d)] + off], d) + t.force(d);
+  };
   auto store = [&](int d, float v) {
     if (d == DC) {
       f[DC * S + n] = St::raw(v + t.force(DC), DC);
       return;
     }
-    const uint32_t dst = reinterpret_cast<const volatile uint32_t*>(e)[d];
+    const uint32_t dst = reinterpret_cast<const volatile uint32_t*>(e)[d] + off;
     const int j = inv(d);
     const bool bounce = dst == static_cast<uint32_t>(j * S + n);
     f[dst] = St::raw(v + (bounce ? t.force(j) : t.force(d)), d);
@@ -85,14 +93,17 @@ __device__ __forceinline__ void batch_odd_node(const BatchTile& T, const uint32_
   trt_update(t, load, store);
 }
 
-constexpr uint32_t kTileAdjBytes = kBatchTileNodes * QM * 4;
+static_assert(kBatchTileNodes == kListTile, "batch tiles are the run records' tiles");
+constexpr uint32_t kRunRecordMax = kRunTileWords * 4;  // largest run record, bytes
+
+__device__ __forceinline__ bool run_bytes_ok(uint32_t bytes) { return bytes > 0 && bytes <= kRunRecordMax; }
 
 // As k_batch_even, with the tile's adjacency staged into shared memory by one
 // bulk copy, double buffered: the copy of the block's next tile is issued
 // before the current tile is updated.
 template <class St>
 __global__ void __launch_bounds__(256) k_batch_odd(const BatchArgs a) {
-  extern __shared__ __align__(128) uint32_t sadj[];  // 2 x kBatchTileNodes x 18
+  extern __shared__ __align__(128) uint32_t sadj[];  // 2 x kRunTileWords
   __shared__ alignas(8) uint64_t bar[2];
   __shared__ __align__(16) BatchTile st[2];
   const int nT = *a.nTiles;
@@ -100,8 +111,16 @@ __global__ void __launch_bounds__(256) k_batch_odd(const BatchArgs a) {
   const bool warp0 = threadIdx.x < 32;
   uint32_t r = 0;
   auto issue = [&](int buf) {  // thread 0, once st[buf] holds the tile's record
-    mbar_arrive_expect_tx(&bar[buf], kTileAdjBytes);
-    bulk_g2s(sadj + buf * kBatchTileNodes * QM, st[buf].adj, kTileAdjBytes, &bar[buf]);
+    // a record that does not fit is not copied: 0 bytes complete the phase
+    // at once, and the tile is skipped below with error bit 4
+    const uint32_t bytes = run_bytes_ok(st[buf].runBytes) ? st[buf].runBytes : 0u;
+    if (bytes) {
+      mbar_arrive_expect_tx(&bar[buf], bytes);
+      bulk_g2s(sadj + buf * kRunTileWords, st[buf].run, bytes, &bar[buf]);
+    } else {
+      atomicOr(a.err, 4);
+      mbar_arrive_expect_tx(&bar[buf], 0);
+    }
   };
   if (warp0) {
     r = tile_load(a.tiles, blockIdx.x);
@@ -135,10 +154,11 @@ __global__ void __launch_bounds__(256) k_batch_odd(const BatchArgs a) {
       return;
     }
     const BatchTile& T = st[buf];
-    const uint32_t* tileAdj = sadj + buf * kBatchTileNodes * QM;
+    if (!run_bytes_ok(T.runBytes)) continue;
+    const uint32_t* srun = sadj + buf * kRunTileWords;
     for (int k = 0; k < a.nodesPerThread; ++k) {
       const int local = threadIdx.x + k * blockDim.x;
-      if (local < T.nValid) batch_odd_node<St>(T, tileAdj + local * QM, T.n0 + local);
+      if (local < T.nValid) batch_odd_node<St>(T, srun, local);
     }
   }
 }
@@ -161,7 +181,7 @@ __global__ void __launch_bounds__(kBatchTileNodes / NPT) k_batch_even_tile(const
 
 template <class St, int NPT>
 __global__ void __launch_bounds__(kBatchTileNodes / NPT) k_batch_odd_tile(const BatchArgs a) {
-  __shared__ __align__(128) uint32_t sadj[kBatchTileNodes * QM];
+  __shared__ __align__(128) uint32_t srun[kRunTileWords];
   __shared__ alignas(8) uint64_t bar;
   __shared__ __align__(16) BatchTile st;
   if (static_cast<int>(blockIdx.x) >= *a.nTiles) return;
@@ -170,11 +190,16 @@ __global__ void __launch_bounds__(kBatchTileNodes / NPT) k_batch_odd_tile(const 
     __syncwarp();
     if (threadIdx.x == 0) {
       mbar_init(&bar, 1);
-      mbar_arrive_expect_tx(&bar, kTileAdjBytes);
-      bulk_g2s(sadj, st.adj, kTileAdjBytes, &bar);
+      if (run_bytes_ok(st.runBytes)) {
+        mbar_arrive_expect_tx(&bar, st.runBytes);
+        bulk_g2s(srun, st.run, st.runBytes, &bar);
+      } else {
+        atomicOr(a.err, 4);
+      }
     }
   }
   __syncthreads();
+  if (!run_bytes_ok(st.runBytes)) return;
   if (!mbar_wait_bounded(&bar, 0)) {
     if (threadIdx.x == 0) atomicOr(a.err, 1);
     return;
@@ -182,7 +207,7 @@ __global__ void __launch_bounds__(kBatchTileNodes / NPT) k_batch_odd_tile(const 
 #pragma unroll 1
   for (int k = 0; k < NPT; ++k) {
     const int local = threadIdx.x + k * (kBatchTileNodes / NPT);
-    if (local < st.nValid) batch_odd_node<St>(st, sadj + local * QM, st.n0 + local);
+    if (local < st.nValid) batch_odd_node<St>(st, srun, local);
   }
 }
 
@@ -201,7 +226,7 @@ static void launch_even(const BatchArgs& a, const BatchLaunch& l, int grid, cuda
 template <class St>
 static void launch_odd(const BatchArgs& a, const BatchLaunch& l, int grid, cudaStream_t s) {
   if (l.blocks > 0)
-    k_batch_odd<St><<<grid, l.threads, 2 * (size_t)kTileAdjBytes, s>>>(a);
+    k_batch_odd<St><<<grid, l.threads, 2 * (size_t)kRunRecordMax, s>>>(a);
   else if (l.nodesPerThread == 4)
     k_batch_odd_tile<St, 4><<<grid, kBatchTileNodes / 4, 0, s>>>(a);
   else if (l.nodesPerThread == 2)
@@ -230,7 +255,9 @@ __global__ void k_batch_tiles(const BatchDomain* doms, const int* tileDom, int n
   const BatchDomain& D = doms[tileDom[t]];
   const int lt = t - D.tileStart;
   BatchTile r;
-  r.adj = D.adj + static_cast<size_t>(lt) * kBatchTileNodes * QM;
+  const uint32_t o0 = D.runOff[lt], o1 = D.runOff[lt + 1];
+  r.run = D.runs + static_cast<size_t>(o0) * 4;
+  r.runBytes = (o1 - o0) * 16u;
   r.f = D.f;
   r.nCells = static_cast<int>(D.nCells);
   r.n0 = lt * kBatchTileNodes;
