@@ -259,6 +259,16 @@ long lbm_b200_launches_for(KernelData *kd, int n);
  * plus a 48-byte header per tile. 0 for the full-array kernels. */
 long long lbm_b200_adjacency_bytes(KernelData *kd);
 
+/* Copies a list instance's run-compressed adjacency to host memory:
+ * tileOffsets (nTiles + 1 entries, 16-byte units; nTiles = ceil(nodes/256))
+ * and records (lbm_b200_adjacency_bytes bytes). Either may be NULL. Per
+ * tile: 8 words of run-head mask (bit k of word w: node 32 w + k of the tile
+ * starts a run), 2 words holding the heads before each mask word (byte w),
+ * 2 zero words, then one 18-entry row per head (even count); node n's link d
+ * is its head's entry d plus n - head. Returns 0, -1 for the full-array
+ * kernels, or a CUDA error code. */
+int lbm_b200_run_records(KernelData *kd, uint32_t *tileOffsets, uint32_t *records);
+
 /* ---- x-slabs of an AA-pattern lattice (one lattice over several GPUs) ----
  * No counterpart in the reference, whose kernels address one array; the
  * slabs reproduce the undivided lattice's run bit for bit.

@@ -197,7 +197,22 @@ __global__ void k_run_fill(const uint32_t* __restrict__ adj, int nFluid, const u
   const int t = blockIdx.x;
   uint32_t* const rec = runs + (size_t)runOff[t] * 4;
   const uint32_t* const m = mask + (size_t)t * (kListTile / 32);
-  if (threadIdx.x < kRunHdrWords) rec[threadIdx.x] = threadIdx.x < kListTile / 32 ? m[threadIdx.x] : 0u;
+  if (threadIdx.x < kRunHdrWords) {
+    uint32_t v = 0u;
+    if (threadIdx.x < kListTile / 32) {
+      v = m[threadIdx.x];
+    } else if (threadIdx.x < kListTile / 32 + 2) {
+      // heads before mask words 4 q .. 4 q + 3, one byte each (at most 224)
+      const int q = threadIdx.x - kListTile / 32;
+      int before = 0;
+      for (int k = 0; k < 4 * q; ++k) before += __popc(m[k]);
+      for (int k = 0; k < 4; ++k) {
+        v |= static_cast<uint32_t>(before) << (8 * k);
+        before += __popc(m[4 * q + k]);
+      }
+    }
+    rec[threadIdx.x] = v;
+  }
   const long long n = (long long)t * kListTile + threadIdx.x;
   if (n >= nFluid) return;
   const int w = threadIdx.x >> 5, b = threadIdx.x & 31;

@@ -60,11 +60,12 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // Stages the run record of tile blockIdx.x (run-compressed adjacency, see
 // kRunHdrWords) into srun (kRunTileWords words) with one bulk copy. A record
 // whose size does not fit flags error bit 4 and is not copied. After the
-// wait, warp 1 prefetches into L2 the record of the tile `a.prefetch` tiles
-// ahead (the block that will take this one's place), off the block's
-// critical path. Returns false (error word set) if the copy did not arrive
-// within the spin limit or was refused; every thread returns the same.
-template <class A>
+// wait, warp 1 prefetches into L2 the record of the tile kWaves x
+// `a.prefetch` tiles ahead (kWaves = 1: the block that will take this one's
+// place), off the block's critical path. Returns false (error word set) if
+// the copy did not arrive within the spin limit or was refused; every thread
+// returns the same.
+template <int kWaves = 1, class A>
 __device__ __forceinline__ bool stage_run_tile(const A& a, uint32_t* srun, uint64_t* bar, int* ok) {
   if (threadIdx.x == 0) {
     const uint32_t o0 = a.runOff[blockIdx.x], o1 = a.runOff[blockIdx.x + 1];
@@ -84,8 +85,8 @@ __device__ __forceinline__ bool stage_run_tile(const A& a, uint32_t* srun, uint6
     if (threadIdx.x == 0) atomicOr(a.err, 1);
     return false;
   }
-  if (threadIdx.x == 32 && a.prefetch > 0 && blockIdx.x + static_cast<unsigned>(a.prefetch) < gridDim.x) {
-    const unsigned t = blockIdx.x + a.prefetch;
+  if (threadIdx.x == 32 && a.prefetch > 0 && blockIdx.x + kWaves * static_cast<unsigned>(a.prefetch) < gridDim.x) {
+    const unsigned t = blockIdx.x + kWaves * a.prefetch;
     const uint32_t o0 = a.runOff[t], o1 = a.runOff[t + 1];
     if (o1 > o0 && (o1 - o0) * 16u <= static_cast<uint32_t>(kRunTileWords) * 4u)
       bulk_prefetch_l2(a.runs + static_cast<size_t>(o0) * 4, (o1 - o0) * 16u);
@@ -97,8 +98,8 @@ __device__ __forceinline__ bool stage_run_tile(const A& a, uint32_t* srun, uint6
 // distance from its run's head: link d of the node is row[d] + off.
 __device__ __forceinline__ const uint32_t* run_row(const uint32_t* srun, int tid, uint32_t& off) {
   const int w = tid >> 5, b = tid & 31;
-  int rank = 0;
-  for (int k = 0; k < w; ++k) rank += __popc(srun[k]);
+  // heads before word w (header byte w of words 8-9), then those up to tid
+  int rank = static_cast<int>((srun[8 + (w >> 2)] >> (8 * (w & 3))) & 0xffu);
   uint32_t mk = srun[w] & ((2u << b) - 1u);
   rank += __popc(mk);
   int k = w;

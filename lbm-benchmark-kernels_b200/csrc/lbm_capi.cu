@@ -955,6 +955,18 @@ const char* lbm_b200_last_error(void) { return g_lastError.c_str(); }
 
 long lbm_b200_launches_for(KernelData* kd, int n) { return launches_for(reinterpret_cast<Gpu*>(kd), n); }
 
+int lbm_b200_run_records(KernelData* kd, uint32_t* tileOffsets, uint32_t* records) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (full_array(g->kind) || !g->dRuns) return -1;
+  cudaError_t e = cudaStreamSynchronize(g->stream);
+  const long long tiles = (g->nFluid + lbm::kListTile - 1) / lbm::kListTile;
+  if (e == cudaSuccess && tileOffsets)
+    e = cudaMemcpy(tileOffsets, g->dRunOff, sizeof(uint32_t) * (size_t)(tiles + 1), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && records) e = cudaMemcpy(records, g->dRuns, g->runBytes, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) g_lastError = cudaGetErrorString(e);
+  return (int)e;
+}
+
 long long lbm_b200_adjacency_bytes(KernelData* kd) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
   if (full_array(g->kind)) return 0;

@@ -73,10 +73,11 @@ constexpr int kListTile = 256;
 // nodes): node n starts a run unless every link of n is the same link of
 // n - 1 plus one, and a tile's first node always starts one. Per tile, at
 // runs + 4 * runOff[t] (16-byte units): a header of kRunHdrWords words (the
-// head mask: bit k of word w = node 32 w + k of the tile starts a run; 4
-// zero words) and one 18-entry row per head, the head count rounded up to
-// even (a multiple of 16 bytes). A node's link d is its head's link d plus
-// its distance from the head.
+// head mask: bit k of word w = node 32 w + k of the tile starts a run; then
+// the heads before each mask word, byte w of words 8-9; 2 zero words) and
+// one 18-entry row per head, the head count rounded up to even (a multiple
+// of 16 bytes). A node's link d is its head's link d plus its distance from
+// the head.
 constexpr int kRunHdrWords = 12;
 constexpr int kRunTileWords = kRunHdrWords + kListTile * 18;
 
