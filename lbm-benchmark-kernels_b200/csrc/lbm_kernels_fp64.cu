@@ -164,27 +164,30 @@ __global__ void __launch_bounds__(128, kDirect ? 7 : 5)
 
 // Cell of shell index i: the x faces (all y, z), then the y faces (inner x,
 // all z), then -- when z is not periodic -- the z faces (inner x and y). A
-// one-cell-thin axis has a single face.
-__device__ __forceinline__ void aa_shell_cell(const AaArgs& a, long long i, int& x, int& y, int& z) {
-  const long long nY = a.nY, nZ = a.nZ;
-  const long long sx = a.nX > 1 ? 2 : 1, sy = a.nY > 1 ? 2 : 1;
-  const long long mx = a.nX > 2 ? a.nX - 2 : 0, my = a.nY > 2 ? a.nY - 2 : 0;
-  const long long nA = sx * nY * nZ, nB = sy * mx * nZ;
+// one-cell-thin axis has a single face. The arithmetic is 32-bit unsigned:
+// the layout holds fewer than 2^31 PDFs, so every product and index here is
+// below 2^31.
+__device__ __forceinline__ void aa_shell_cell(const AaArgs& a, long long i64, int& x, int& y, int& z) {
+  const unsigned i = static_cast<unsigned>(i64);
+  const unsigned nY = a.nY, nZ = a.nZ;
+  const unsigned sx = a.nX > 1 ? 2 : 1, sy = a.nY > 1 ? 2 : 1;
+  const unsigned mx = a.nX > 2 ? a.nX - 2 : 0, my = a.nY > 2 ? a.nY - 2 : 0;
+  const unsigned nA = sx * nY * nZ, nB = sy * mx * nZ;
   if (i < nA) {
     x = (i / (nY * nZ)) == 0 ? 0 : a.nX - 1;
-    const long long r = i % (nY * nZ);
+    const unsigned r = i % (nY * nZ);
     y = (int)(r / nZ);
     z = (int)(r % nZ);
   } else if (i < nA + nB) {
-    const long long j = i - nA;
+    const unsigned j = i - nA;
     y = (j / (mx * nZ)) == 0 ? 0 : a.nY - 1;
-    const long long r = j % (mx * nZ);
+    const unsigned r = j % (mx * nZ);
     x = 1 + (int)(r / nZ);
     z = (int)(r % nZ);
   } else {
-    const long long k = i - nA - nB;
+    const unsigned k = i - nA - nB;
     z = (k / (mx * my)) == 0 ? 0 : a.nZ - 1;
-    const long long r = k % (mx * my);
+    const unsigned r = k % (mx * my);
     x = 1 + (int)(r / my);
     y = 1 + (int)(r % my);
   }
