@@ -360,6 +360,14 @@ __global__ void __launch_bounds__(128) k_fa_pull_fp64(const AaArgs a, const Trt<
   const double* const f = a.f;
   double* const g = launder(a.g);
   auto load = [&](int d) -> double { return f[d * S + c - aa_off(a, d)]; };
+  // a cell off every face with all links direct has no periodic image, wall
+  // or open-face slot to write: its 19 stores are its own slots (the check is
+  // uniform across most warps; 0.946 -> 0.896 ms per step at 256^3)
+  const bool inner = !(w & kLinkBits) && x > 0 && x < a.nX - 1 && y > 0 && y < a.nY - 1 && z > 0 && z < a.nZ - 1;
+  if (inner) {
+    trt_update(t, load, [&](int e, double v) { g[e * S + c] = v + t.force[e]; });
+    return;
+  }
   auto store = [&](int e, double v) {
     g[e * S + c] = v + t.force[e];
     if (e == DC) return;
