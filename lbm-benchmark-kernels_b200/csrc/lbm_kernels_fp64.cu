@@ -325,6 +325,14 @@ __global__ void __launch_bounds__(128) k_fa_push_fp64(const AaArgs a, const Trt<
   const long long S = a.dstride;
   const double* const f = a.f + c;
   double* const g = launder(a.g);
+  // a cell off every face with all links direct writes each PDF to x + c_d
+  // without wrap or bounce logic (a warp-uniform branch for most warps)
+  const bool inner = !(w & kLinkBits) && x > 0 && x < a.nX - 1 && y > 0 && y < a.nY - 1 && z > 0 && z < a.nZ - 1;
+  if (inner) {
+    trt_update(t, [&](int d) { return f[d * S]; },
+               [&](int d, double v) { g[d * S + c + aa_off(a, d)] = v + t.force[d]; });
+    return;
+  }
   auto store = [&](int d, double v) {
     if (d == DC) {
       g[DC * S + c] = v + t.force[DC];
