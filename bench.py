@@ -280,7 +280,7 @@ def cpu_model():
 
 
 # ---------------------------------------------------------------------------
-# BASELINE configs[3..4] and configs[2]: batched, served, reduced precision
+# the batched (512 domains), served and reduced-precision workloads
 
 def _batch_domains(n, seed, edge_range=(32, 128), threads=16):
     """n seeded porous domains: edge U{32..128}, r ~ U[3,8], porosity U[0.3,0.6],

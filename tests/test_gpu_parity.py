@@ -5,7 +5,7 @@ FP64 kernels are compiled without FMA contraction and evaluate the collision
 in the reference's scalar order, so the fields must equal the CPU oracle bit
 for bit, and the reference's scalar aa-soa kernel bit for bit; the reference's
 SIMD list kernels differ from their own scalar path in rounding, so against
-them the bound is 1e-13 relative (the north-star tolerance is 1e-12)."""
+them the bound is 1e-13 relative (the required bound is 1e-12)."""
 import zlib
 
 import numpy as np
