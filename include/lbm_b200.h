@@ -283,18 +283,20 @@ int lbm_b200_run_records(KernelData *kd, uint32_t *tileOffsets, uint32_t *record
  * errors (lbm_b200_last_error).
  *
  * lbm_aa_list_slab_init: the same for the list AA kernel
- * (cuda-list-aa-pv-soa, FP64 storage): the slab's fluid cells are the owned
- * nodes (the kernel's blocked numbering over the slab), followed by ghost
- * nodes for the fluid cells of the neighbouring slabs that owned links reach;
- * adjacency follows the whole lattice's link rule.
+ * (cuda-list-aa-pv-soa, any -precision): the slab's fluid cells are the
+ * owned nodes (the kernel's blocked numbering over the slab), followed by
+ * ghost nodes for the fluid cells of the neighbouring slabs that owned links
+ * reach; adjacency follows the whole lattice's link rule.
  *
  * A step pair is: lbm_aa_slab_step(half 0, even step) on every slab; for
  * every halo face, lbm_aa_halo_pack(side, 0) -> send to the neighbour ->
  * lbm_aa_halo_unpack(side, 0) there; lbm_aa_slab_step(half 1, odd step); the
  * same exchange with phase 1. side 0 is the x0 face, 1 the x1-1 face.
  * Pack of (side 1, phase p) pairs with unpack of (side 0, phase p) on the
- * right-hand neighbour and vice versa. Messages are doubles in device
- * memory: lbm_aa_halo_message(side, phase, send) of them go out (send = 1)
+ * right-hand neighbour and vice versa. Messages are PDF elements in device
+ * memory, in the slab's storage format moved bit for bit
+ * (lbm_aa_halo_elem_bytes: 8 for FP64, 4 or 2 for the FP32 / FP16 list
+ * storage): lbm_aa_halo_message(side, phase, send) of them go out (send = 1)
  * or come in (send = 0) through a face -- 5 x nY x nZ for full-array slabs,
  * the face's link count for list slabs (-1: no halo on that face);
  * lbm_aa_halo_count is the largest message of the slab. The functions
@@ -306,8 +308,9 @@ KernelData *lbm_aa_list_slab_init(LatticeDesc *global, int x0, int x1, int haloL
 void lbm_aa_slab_deinit(KernelData *kd);
 long long lbm_aa_halo_count(KernelData *kd);
 long long lbm_aa_halo_message(KernelData *kd, int side, int phase, int send);
-int lbm_aa_halo_pack(KernelData *kd, int side, int phase, double *buf, void *stream);
-int lbm_aa_halo_unpack(KernelData *kd, int side, int phase, const double *buf, void *stream);
+int lbm_aa_halo_elem_bytes(KernelData *kd);
+int lbm_aa_halo_pack(KernelData *kd, int side, int phase, void *buf, void *stream);
+int lbm_aa_halo_unpack(KernelData *kd, int side, int phase, const void *buf, void *stream);
 int lbm_aa_slab_step(KernelData *kd, CaseData *cd, int half, void *stream);
 
 /* The layout lbm_aa_list_slab_init builds, on the host only (no CUDA call):

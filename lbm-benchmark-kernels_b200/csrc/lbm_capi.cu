@@ -1036,13 +1036,11 @@ static const char* list_slab_error(int rc) {
 
 KernelData* lbm_aa_list_slab_init(LatticeDesc* global, int x0, int x1, int haloLo, int haloHi, Parameters* params) {
   const Args a = parse_args(params);
-  if (a.storage != lbm::kStoreF64) {
-    g_lastError = "list slabs store FP64 PDFs";
-    return nullptr;
-  }
   LbmhListSlab ls;
   const int halo[2] = {haloLo != 0, haloHi != 0};
-  const int rc = lbmh_list_slab_build(global, x0, x1, halo, a.blk, a.pad, &ls);
+  // reduced storage: planes padded to whole staging tiles, as for an instance
+  const int quantum = a.storage == lbm::kStoreF64 ? 0 : lbm::kLpTileNodes;
+  const int rc = lbmh_list_slab_build(global, x0, x1, halo, a.blk, a.pad, quantum, &ls);
   if (rc) {
     g_lastError = list_slab_error(rc);
     return nullptr;
@@ -1067,7 +1065,8 @@ int lbm_aa_list_slab_layout(const LatticeDesc* global, int x0, int x1, int haloL
   const Args a = parse_args(params);
   LbmhListSlab ls;
   const int halo[2] = {haloLo != 0, haloHi != 0};
-  const int rc = lbmh_list_slab_build(global, x0, x1, halo, a.blk, a.pad, &ls);
+  const int quantum = a.storage == lbm::kStoreF64 ? 0 : lbm::kLpTileNodes;
+  const int rc = lbmh_list_slab_build(global, x0, x1, halo, a.blk, a.pad, quantum, &ls);
   if (rc) {
     g_lastError = list_slab_error(rc);
     return rc;
@@ -1132,35 +1131,39 @@ static int list_halo_list(Gpu* g, int side, int phase, bool pack) {
   return g->nHalo[side][list] < 0 ? -1 : list;
 }
 
-int lbm_aa_halo_pack(KernelData* kd, int side, int phase, double* buf, void* stream) {
+int lbm_aa_halo_elem_bytes(KernelData* kd) { return (int)reinterpret_cast<Gpu*>(kd)->elemBytes; }
+
+int lbm_aa_halo_pack(KernelData* kd, int side, int phase, void* buf, void* stream) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
   if (side < 0 || side > 1 || phase < 0 || phase > 1) return -1;
   if (g->listSlab) {
     const int list = list_halo_list(g, side, phase, true);
     if (list < 0) return -1;
     sync_upload(g);
-    lbm::slot_gather(g->dF, g->dHalo[side][list], g->nHalo[side][list], buf, stream_or(g, stream));
+    lbm::slot_gather(g->dF, g->dHalo[side][list], g->nHalo[side][list], buf, (int)g->elemBytes,
+                     stream_or(g, stream));
     return (int)cudaGetLastError();
   }
   if (g->kind != kAa) return -1;
   sync_upload(g);
-  lbm::aa_halo_pack(aa_args(g), side, phase, buf, stream_or(g, stream));
+  lbm::aa_halo_pack(aa_args(g), side, phase, static_cast<double*>(buf), stream_or(g, stream));
   return (int)cudaGetLastError();
 }
 
-int lbm_aa_halo_unpack(KernelData* kd, int side, int phase, const double* buf, void* stream) {
+int lbm_aa_halo_unpack(KernelData* kd, int side, int phase, const void* buf, void* stream) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
   if (side < 0 || side > 1 || phase < 0 || phase > 1) return -1;
   if (g->listSlab) {
     const int list = list_halo_list(g, side, phase, false);
     if (list < 0) return -1;
     sync_upload(g);
-    lbm::slot_scatter(g->dF, g->dHalo[side][list], g->nHalo[side][list], buf, stream_or(g, stream));
+    lbm::slot_scatter(g->dF, g->dHalo[side][list], g->nHalo[side][list], buf, (int)g->elemBytes,
+                      stream_or(g, stream));
     return (int)cudaGetLastError();
   }
   if (g->kind != kAa) return -1;
   sync_upload(g);
-  lbm::aa_halo_unpack(aa_args(g), side, phase, buf, stream_or(g, stream));
+  lbm::aa_halo_unpack(aa_args(g), side, phase, static_cast<const double*>(buf), stream_or(g, stream));
   return (int)cudaGetLastError();
 }
 
@@ -1170,6 +1173,17 @@ int lbm_aa_slab_step(KernelData* kd, CaseData* cd, int half, void* stream) {
   sync_upload(g);
   const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
   const cudaStream_t s = stream_or(g, stream);
+  if (g->listSlab && g->storage != lbm::kStoreF64) {
+    const lbm::ListArgsLp la = list_args_lp(g);
+    const lbm::Trt<float> tf = to_float(t);
+    if (half == 0) {
+      lbm::list_even_lp(la, tf, g->storage, s);
+    } else {
+      lbm::list_odd_lp(la, tf, g->storage, s);
+      g->iteration += 2;
+    }
+    return (int)cudaGetLastError();
+  }
   if (g->listSlab) {
     const lbm::ListArgs la = list_args(g);
     if (half == 0) {

@@ -297,7 +297,7 @@ void lbmh_list_slab_free(LbmhListSlab *s)
 #define SLAB_CELLS_END }}
 
 int lbmh_list_slab_build(const LatticeDesc *ld, int x0, int x1, const int halo[2], const int blk[3],
-                         const char *pad, LbmhListSlab *s)
+                         const char *pad, int quantum, LbmhListSlab *s)
 {
 	const int nx = ld->Dims[0], ny = ld->Dims[1], nz = ld->Dims[2];
 	const int L = x1 - x0;
@@ -339,7 +339,12 @@ int lbmh_list_slab_build(const LatticeDesc *ld, int x0, int x1, const int halo[2
 		}
 	SLAB_CELLS_END
 	s->nGhost = nGhost;
-	s->nCells = lbmh_pad_cells(s->nOwned + nGhost, (int)sizeof(double), pad);
+	if (quantum > 0) {
+		const long n = s->nOwned + nGhost > 0 ? s->nOwned + nGhost : 1;
+		s->nCells = (int)((n + quantum - 1) / quantum * quantum);
+	} else {
+		s->nCells = lbmh_pad_cells(s->nOwned + nGhost, (int)sizeof(double), pad);
+	}
 	if (s->nCells < 0) { rc = -4; goto done; }
 	if ((uint64_t)19 * (uint64_t)s->nCells >= (1ull << 32)) { rc = -5; goto done; }
 	const uint32_t nc = (uint32_t)s->nCells;

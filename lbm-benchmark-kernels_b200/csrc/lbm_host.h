@@ -51,11 +51,14 @@ typedef struct {
 } LbmhListSlab;
 
 /* Builds the slab layout (halo[side] = 1: that face has a neighbour slab).
+ * nCells: the owned and ghost nodes padded as the reference pads a list
+ * (pad string, 8-byte PDFs) when quantum is 0, else rounded up to a multiple
+ * of quantum (the reduced-storage layout's whole staging tiles).
  * Returns 0; -1 bad range (or a halo on a slab that spans the lattice);
  * -2 a link leaves through a face without a halo; -3 allocation failure;
  * -4 malformed padding string; -5 more PDFs than 32-bit indices address. */
 int lbmh_list_slab_build(const LatticeDesc *ld, int x0, int x1, const int halo[2], const int blk[3],
-                         const char *pad, LbmhListSlab *s);
+                         const char *pad, int quantum, LbmhListSlab *s);
 void lbmh_list_slab_free(LbmhListSlab *s);
 
 /* Link words of the full-array AA layout: for every cell of the padded

@@ -142,9 +142,10 @@ long long list_build_device(const int* mask, const int dims[3], const int period
                             const char** err);
 
 // Halo messages of a list slab: buf[k] = f[idx[k]] (gather) and
-// f[idx[k]] = buf[k] (scatter) for k < n.
-void slot_gather(const double* f, const uint32_t* idx, long long n, double* buf, cudaStream_t s);
-void slot_scatter(double* f, const uint32_t* idx, long long n, const double* buf, cudaStream_t s);
+// f[idx[k]] = buf[k] (scatter) for k < n, elements of elemBytes (8, 4 or 2:
+// the slab's PDF storage) moved bit for bit.
+void slot_gather(const void* f, const uint32_t* idx, long long n, void* buf, int elemBytes, cudaStream_t s);
+void slot_scatter(void* f, const uint32_t* idx, long long n, const void* buf, int elemBytes, cudaStream_t s);
 
 // Run-compressed adjacency of the nFluid nodes of adj (device, 18 entries
 // per node): allocates *runs (cudaMalloc, *runBytes bytes) and *runOff

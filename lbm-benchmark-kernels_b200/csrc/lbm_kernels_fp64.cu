@@ -578,24 +578,46 @@ __global__ void __launch_bounds__(kListTile, 3) k_list_push_fp64(const ListArgs 
   trt_update(t, [&](int d) { return f[d * S]; }, store);
 }
 
-__global__ void k_slot_gather(const double* __restrict__ f, const uint32_t* __restrict__ idx, long long n,
-                              double* __restrict__ buf) {
+template <typename E>
+__global__ void k_slot_gather(const E* __restrict__ f, const uint32_t* __restrict__ idx, long long n,
+                              E* __restrict__ buf) {
   const long long k = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (k < n) buf[k] = f[idx[k]];
 }
 
-__global__ void k_slot_scatter(double* __restrict__ f, const uint32_t* __restrict__ idx, long long n,
-                               const double* __restrict__ buf) {
+template <typename E>
+__global__ void k_slot_scatter(E* __restrict__ f, const uint32_t* __restrict__ idx, long long n,
+                               const E* __restrict__ buf) {
   const long long k = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (k < n) f[idx[k]] = buf[k];
 }
 
-void slot_gather(const double* f, const uint32_t* idx, long long n, double* buf, cudaStream_t s) {
-  if (n > 0) k_slot_gather<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(f, idx, n, buf);
+template <typename E>
+static void slot_move(bool gather, void* f, const uint32_t* idx, long long n, void* buf, cudaStream_t s) {
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  if (gather)
+    k_slot_gather<E><<<blocks, 256, 0, s>>>(static_cast<const E*>(f), idx, n, static_cast<E*>(buf));
+  else
+    k_slot_scatter<E><<<blocks, 256, 0, s>>>(static_cast<E*>(f), idx, n, static_cast<const E*>(buf));
 }
 
-void slot_scatter(double* f, const uint32_t* idx, long long n, const double* buf, cudaStream_t s) {
-  if (n > 0) k_slot_scatter<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(f, idx, n, buf);
+static void slot_move_bytes(bool gather, void* f, const uint32_t* idx, long long n, void* buf, int elemBytes,
+                            cudaStream_t s) {
+  if (n <= 0) return;
+  if (elemBytes == 8)
+    slot_move<unsigned long long>(gather, f, idx, n, buf, s);
+  else if (elemBytes == 4)
+    slot_move<unsigned int>(gather, f, idx, n, buf, s);
+  else if (elemBytes == 2)
+    slot_move<unsigned short>(gather, f, idx, n, buf, s);
+}
+
+void slot_gather(const void* f, const uint32_t* idx, long long n, void* buf, int elemBytes, cudaStream_t s) {
+  slot_move_bytes(true, const_cast<void*>(f), idx, n, buf, elemBytes, s);
+}
+
+void slot_scatter(void* f, const uint32_t* idx, long long n, const void* buf, int elemBytes, cudaStream_t s) {
+  slot_move_bytes(false, f, idx, n, const_cast<void*>(buf), elemBytes, s);
 }
 
 static unsigned list_blocks(const ListArgs& a) { return (a.nFluid + kListTile - 1) / kListTile; }

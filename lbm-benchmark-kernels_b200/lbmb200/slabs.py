@@ -19,8 +19,9 @@ A step pair of the AA pattern on a slab:
 Every slot is read and written by exactly one cell in the odd step, so after
 the pair the slabs hold the whole lattice's state bit for bit (tested against
 the single-instance kernel). Messages are 5 x nY x nZ doubles per face and
-phase for full-array slabs, one double per link through the face for list
-slabs (``Slab.message``).
+phase for full-array slabs, one PDF element (8, 4 or 2 bytes: the list's
+storage) per link through the face for list slabs (``Slab.message``); the
+transports carry them in buffers of 8-byte words.
 
 Transports: ``LocalTransport`` (all slabs in this process: device-to-device
 through shared device buffers, every operation on one stream) and
@@ -75,6 +76,7 @@ def _sigs(L):
         L.lbm_aa_halo_count.restype = ctypes.c_longlong
         L.lbm_aa_halo_message.restype = ctypes.c_longlong
         L.lbm_aa_halo_message.argtypes = [ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.lbm_aa_halo_elem_bytes.argtypes = [ctypes.POINTER(KernelData)]
         L.lbm_aa_list_slab_layout.argtypes = [ctypes.POINTER(LatticeDesc), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                               ctypes.c_int, ctypes.POINTER(Parameters),
                                               ctypes.POINTER(ctypes.c_longlong)] + [ctypes.c_void_p] * 6
@@ -121,11 +123,12 @@ class Slab:
             raise RuntimeError("slab init failed: %s" % self.L.lbm_b200_last_error().decode())
         self.inst = Instance(None, self.local, kdp)
         self.kdp = kdp
+        self.elem_bytes = int(self.L.lbm_aa_halo_elem_bytes(kdp))
         self.count = int(self.L.lbm_aa_halo_count(kdp))
 
     def message(self, side, phase, send):
-        """Doubles this slab sends (send=True) or receives through `side` in
-        `phase` (-1: no halo on that face)."""
+        """PDF elements (elem_bytes each) this slab sends (send=True) or
+        receives through `side` in `phase` (-1: no halo on that face)."""
         return int(self.L.lbm_aa_halo_message(self.kdp, int(side), int(phase), int(bool(send))))
 
     def step(self, cd, half, stream=None):
@@ -150,10 +153,19 @@ class Slab:
 
 
 def message(slab, side, phase, send):
-    """Length of a slab's message through `side` in `phase`: the slab's own
-    ``message`` method, else its fixed ``count``."""
+    """Length of a slab's message through `side` in `phase`, in 8-byte words
+    (the transports' buffers hold doubles; a message of 4- or 2-byte PDF
+    elements fills the words' leading bytes): the slab's own ``message``
+    method, else its fixed ``count``; -1 without a halo."""
     m = getattr(slab, "message", None)
-    return m(side, phase, send) if m else slab.count
+    n = m(side, phase, send) if m else slab.count
+    return n if n < 0 else words(slab, n)
+
+
+def words(slab, n):
+    """8-byte words holding n PDF elements of the slab's storage."""
+    eb = getattr(slab, "elem_bytes", 8)
+    return (n * eb + 7) // 8
 
 
 class LocalTransport:
@@ -175,7 +187,8 @@ class LocalTransport:
                 if (message(slabs[r], 1, phase, True) != message(slabs[q], 0, phase, False)
                         or message(slabs[q], 0, phase, True) != message(slabs[r], 1, phase, False)):
                     raise ValueError("slabs %d and %d disagree on their shared face's messages" % (r, q))
-        self.bufs = {f: (alloc(max(1, slabs[f[0]].count)), alloc(max(1, slabs[f[1]].count))) for f in self.faces}
+        self.bufs = {f: (alloc(max(1, words(slabs[f[0]], slabs[f[0]].count))),
+                         alloc(max(1, words(slabs[f[1]], slabs[f[1]].count)))) for f in self.faces}
 
     def exchange(self, phase):
         for (r, q) in self.faces:

@@ -143,3 +143,30 @@ def test_slabrun_list_layout_single_process(capsys):
     # the flow starts at rest with f = w: the mass is one per fluid node
     assert abs(rec["sum_rho"] - rec["fluid_nodes"]) < 1e-9 * rec["fluid_nodes"]
     assert rec["sum_jx"] > 0 and rec["permeability"] > 0
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+@pytest.mark.parametrize("geo,dims,per,parts", [
+    ("spheres", (30, 24, 24), (1, 1, 1), 3),
+    ("channel", (30, 12, 14), (0, 0, 0), 3),
+    ("fluid", (9, 8, 7), (0, 1, 0), 3),
+])
+def test_reduced_storage_list_slabs_equal_whole_lattice(prec, geo, dims, per, parts):
+    """FP32 / FP16 list slabs: halo messages carry the stored elements bit for
+    bit, so the slabs equal the single reduced-storage instance exactly."""
+    lat = _lattice(geo, dims, per)
+    rng = np.random.default_rng(3)
+    w = lbmb200.W
+    init = w[None, :] * (1.0 + 0.05 * (rng.random((lat.mask.size, 19)) - 0.5))
+    cd = lbmb200.case(omega=1.1, xforce=2e-4, iterations=10)
+    kargs = ["-lambda", "3/16", "-precision", prec]
+    inst = lbmb200.kernel("cuda-list-aa-pv-soa").init(lat, kernel_args=kargs)
+    try:
+        inst.set_field(init)
+        inst.run(cd)
+        whole = inst.get_field()
+    finally:
+        inst.deinit()
+    got = _run_slabs(lat, parts, init, cd, 5, layout="list", kargs=kargs)
+    m = lat.mask != 0
+    assert np.array_equal(got[m], whole[m])

@@ -26,6 +26,7 @@ CASES = [
     ("blocks-2", (8, 8, 8), (1, 0, 1), 4, ("-pad", "no")),
     ("fluid", (5, 4, 4), (1, 1, 1), 4, ("-pad", "no")),         # slabs of one and two planes
     ("fluid", (3, 4, 5), (1, 0, 0), 3, ("-pad", "no")),         # one plane per slab, periodic x only
+    ("channel", (10, 7, 6), (1, 1, 0), 3, ("-precision", "fp32")),  # reduced-storage layout: whole 1024-node tiles
 ]
 
 
@@ -106,3 +107,11 @@ def test_closed_face_refuses_crossing_link():
     lat = lbmb200.geometry("fluid", (6, 4, 4), (1, 1, 1))
     with pytest.raises(RuntimeError, match="without a halo"):
         sl.list_slab_layout(lat, 0, 3, False, True)
+
+
+def test_reduced_storage_layout_pads_to_tiles():
+    lat = lbmb200.geometry("fluid", (9, 6, 5), (1, 1, 1))
+    for r, (x0, x1) in enumerate(sl.partition(9, 3)):
+        lo, hi = sl.halo_flags(r, 3, True)
+        lay = sl.list_slab_layout(lat, x0, x1, lo, hi, ("-precision", "fp16"))
+        assert lay["n_cells"] % 1024 == 0 and lay["n_cells"] >= lay["n_owned"] + lay["n_ghost"]
