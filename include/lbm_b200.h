@@ -351,9 +351,10 @@ int lbm_b200_device_state(KernelData *kd, double **pdfs, long long *nCells, int 
  * Synchronises the stream. Returns 0, or a CUDA error code / -1. */
 int lbm_b200_moments_device(const double *pdfs, long long nCells, int nFluid, double *out_device, void *stream);
 
-/* The same sums for an FP64 list-kernel instance, into host memory
- * (out[0..3]); waits for the instance's pending steps. Returns 0, -1 for the
- * full-array kernel or reduced storage, or a CUDA error code. */
+/* The same sums for a list-kernel instance, into host memory (out[0..3]);
+ * waits for the instance's pending steps. With FP32/FP16 storage the stored
+ * deviations from the weights are summed in FP64 and the node count added to
+ * the mass. Returns 0, -1 for the full-array kernels, or a CUDA error code. */
 int lbm_b200_instance_moments(KernelData *kd, double *out);
 
 /* Checkpoint / restart of an instance (no counterpart in the reference):

@@ -90,6 +90,7 @@ struct Gpu {
   int cur;  // pull: index of the current grid (0 = dF, 1 = dG)
 
   double* dMomOut;  // 4 doubles for lbm_b200_instance_moments (allocated on first use)
+  double* dMomPartials;  // its per-block partial sums for reduced storage (first use)
 
   // last Kernel call
   double lastDeviceMs;
@@ -771,6 +772,7 @@ void gpu_free(KernelData** kernelData) {
     for (int list = 0; list < 2; ++list) cudaFree(g->dHalo[side][list]);
   cudaFree(g->dErr);
   cudaFree(g->dMomOut);
+  cudaFree(g->dMomPartials);
   cudaFreeHost(g->mirror);
   cudaFreeHost(g->rawStage);
   cudaEventDestroy(g->ev0);
@@ -1315,11 +1317,25 @@ int lbm_b200_moments_device(const double* pdfs, long long nCells, int nFluid, do
 
 int lbm_b200_instance_moments(KernelData* kd, double* out) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
-  if (full_array(g->kind) || g->storage != lbm::kStoreF64) return -1;
+  if (full_array(g->kind)) return -1;
   if (g->dirty) upload_if_dirty(g);
   if (g->dMomOut == nullptr) {
     cudaError_t e = cudaMalloc(&g->dMomOut, 4 * sizeof(double));
     if (e != cudaSuccess) { g_lastError = cudaGetErrorString(e); return (int)e; }
+  }
+  if (g->storage != lbm::kStoreF64) {
+    // reduced storage: FP64 sums of the stored deviations (scratch kept by
+    // the instance)
+    if (g->dMomPartials == nullptr) {
+      cudaError_t e = cudaMalloc(&g->dMomPartials, sizeof(double) * 4 * lbm::moment_blocks(g->nFluid));
+      if (e != cudaSuccess) { g_lastError = cudaGetErrorString(e); return (int)e; }
+    }
+    lbm::moments_enqueue_lp(g->dF, g->storage, g->nCells, g->nFluid, g->dMomPartials, g->dMomOut, g->stream);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(out, g->dMomOut, 4 * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) g_lastError = cudaGetErrorString(e);
+    return (int)e;
   }
   int rc = lbm_b200_moments_device(current_grid(g), g->nCells, g->nFluid, g->dMomOut, g->stream);
   if (rc) return rc;

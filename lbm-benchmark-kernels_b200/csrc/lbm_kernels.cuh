@@ -187,5 +187,8 @@ void list_push_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
 // {sum rho, sum j_x, sum j_y, sum j_z}.
 int moment_blocks(int nFluid);
 void moments_enqueue(const double* f, long long nCells, int nFluid, double* partials, double* out, cudaStream_t s);
+// The same sums over reduced storage (kStoreF32 / kStoreF16 deviations).
+void moments_enqueue_lp(const void* f, int storage, long long nCells, int nFluid, double* partials, double* out,
+                        cudaStream_t s);
 
 }  // namespace lbm

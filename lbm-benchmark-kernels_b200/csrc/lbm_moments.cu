@@ -10,6 +10,7 @@
 // The entry point allocates the scratch (4 doubles per block) with cudaMalloc
 // for each call.
 #include "lbm_kernels.cuh"
+#include "lbm_store.cuh"
 
 namespace lbm {
 
@@ -79,6 +80,46 @@ void moments_enqueue(const double* f, long long nCells, int nFluid, double* part
   const int nb = moment_blocks(nFluid);
   k_moments_partial<<<nb, kMomentTile, 0, s>>>(f, nCells, nFluid, partials);
   k_moments_final<<<1, kMomentTile, 0, s>>>(partials, nb, out);
+}
+
+// Reduced storage (FP32 or FP16 deviations delta_i = f_i - w_i): per node,
+// sum_i delta_i (= rho - 1) and the momentum sum_i c_i delta_i (the weights'
+// momentum vanishes), each stored element converted exactly to FP64; pass 2
+// adds nFluid to the mass, so out[0] = sum rho as for FP64 storage.
+template <class St>
+__global__ void __launch_bounds__(kMomentTile) k_moments_partial_lp(const void* fv, long long nCells, int nFluid,
+                                                                    double* partials) {
+  using Elem = typename St::T;
+  const Elem* f = static_cast<const Elem*>(fv);
+  const int n = blockIdx.x * kMomentTile + threadIdx.x;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  if (n < nFluid) {
+    double v[Q];
+#pragma unroll
+    for (int d = 0; d < Q; ++d) v[d] = static_cast<double>(St::dev(f[d * nCells + n], d));
+    s[0] = v[C] + v[N] + v[E] + v[S] + v[W] + v[NE] + v[SE] + v[SW] + v[NW] + v[T] + v[TN] + v[TE] + v[TS] + v[TW] +
+           v[B] + v[BN] + v[BE] + v[BS] + v[BW];
+    s[1] = v[E] + v[NE] + v[SE] + v[TE] + v[BE] - v[W] - v[NW] - v[SW] - v[TW] - v[BW];
+    s[2] = v[N] + v[NE] + v[NW] + v[TN] + v[BN] - v[S] - v[SE] - v[SW] - v[TS] - v[BS];
+    s[3] = v[T] + v[TE] + v[TW] + v[TN] + v[TS] - v[B] - v[BE] - v[BW] - v[BN] - v[BS];
+  }
+  block_sum4(s);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) partials[blockIdx.x * 4 + k] = s[k];
+}
+
+__global__ void k_moments_add_mass(double* out, int nFluid) { out[0] = static_cast<double>(nFluid) + out[0]; }
+
+void moments_enqueue_lp(const void* f, int storage, long long nCells, int nFluid, double* partials, double* out,
+                        cudaStream_t s) {
+  const int nb = moment_blocks(nFluid);
+  if (storage == kStoreF16)
+    k_moments_partial_lp<StoreF16><<<nb, kMomentTile, 0, s>>>(f, nCells, nFluid, partials);
+  else
+    k_moments_partial_lp<StoreF32><<<nb, kMomentTile, 0, s>>>(f, nCells, nFluid, partials);
+  k_moments_final<<<1, kMomentTile, 0, s>>>(partials, nb, out);
+  k_moments_add_mass<<<1, 1, 0, s>>>(out, nFluid);
 }
 
 }  // namespace lbm

@@ -298,7 +298,7 @@ class Instance:
 
     def moments(self):
         """lbm_b200_instance_moments: FP64 (sum rho, sum j_x, sum j_y, sum j_z)
-        over the instance's fluid nodes (FP64 list kernels)."""
+        over the instance's fluid nodes (list kernels, any storage)."""
         out = (ctypes.c_double * 4)()
         rc = lib().lbm_b200_instance_moments(self.kdp, out)
         if rc:

@@ -10,8 +10,9 @@ per GPU, halo messages through torch.distributed (NCCL):
 same lattice, takes its slab -- full array (cuda-aa-soa kernels) or fluid-node
 list (cuda-list-aa-pv-soa kernels) -- and runs `pairs` even/odd step pairs;
 rank 0 prints the aggregate MFLUP/s (device-timed per rank with CUDA events,
-max over ranks). List slabs also report the FP64 conservation sums of the
-whole lattice (per-slab sums all-reduced) and the permeability they give.
+max over ranks). List slabs (any --precision) also report the FP64
+conservation sums of the whole lattice (per-slab sums all-reduced) and the
+permeability they give.
 With one process, the lattice runs as one slab without halos.
 """
 import argparse
@@ -30,6 +31,8 @@ def main(argv=None):
     p.add_argument("--omega", type=float, default=1.0)
     p.add_argument("--lambda", dest="lam", default="3/16")
     p.add_argument("--layout", default="full", choices=("full", "list"))
+    p.add_argument("--precision", default="fp64", choices=("fp64", "fp32", "fp16"),
+                   help="PDF storage of list slabs")
     a = p.parse_args(argv)
 
     import torch
@@ -49,7 +52,10 @@ def main(argv=None):
         lo, hi = sl.halo_flags(ranks.rank, ranks.world, ring)
         lbmb200.lib().lbm_b200_set_device(ranks.local)
         torch.cuda.set_device(ranks.local)
-        slab = sl.Slab(lat, x0, x1, lo, hi, kernel_args=["-lambda", a.lam], layout=a.layout)
+        if a.precision != "fp64" and a.layout != "list":
+            raise SystemExit("--precision fp32/fp16 needs --layout list")
+        kargs = ["-lambda", a.lam] + (["-precision", a.precision] if a.layout == "list" else [])
+        slab = sl.Slab(lat, x0, x1, lo, hi, kernel_args=kargs, layout=a.layout)
         if a.layout == "list":
             slab.inst.set_field(np.broadcast_to(lbmb200.W, (slab.local.mask.size, 19)))
         # an explicit stream, current for torch.distributed too: kernels,
@@ -70,7 +76,8 @@ def main(argv=None):
         torch.cuda.synchronize()
         ms = ranks.max(e0.elapsed_time(e1))
         nodes = ranks.sum(slab.local.n_fluid)
-        rec = {"dims": dims, "geometry": a.geometry, "layout": a.layout, "ranks": ranks.world,
+        rec = {"dims": dims, "geometry": a.geometry, "layout": a.layout, "precision": a.precision,
+               "ranks": ranks.world,
                "fluid_nodes": nodes, "pairs": a.pairs, "ms": round(ms, 3),
                "mflups": round(nodes * 2 * a.pairs / (ms / 1e3) / 1e6, 1)}
         if a.layout == "list":

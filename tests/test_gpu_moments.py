@@ -56,3 +56,24 @@ def test_moments_deterministic():
     finally:
         inst.deinit()
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_reduced_storage_instance_moments(prec):
+    """lbm_b200_instance_moments on FP32/FP16 storage: FP64 sums of the stored
+    deviations plus the node count, against the host sums of the field the
+    instance hands back through GetNode (weights plus the same deviations)."""
+    lat, _ = lbmb200.spheres((28, 24, 20), 4, 0.5, 2.0, 4.0, 3000)
+    inst = lbmb200.kernel("cuda-list-aa-pv-soa").init(lat, kernel_args=["-precision", prec])
+    try:
+        rng = np.random.default_rng(2)
+        inst.set_field(lbmb200.W[None, :] * (1.0 + 0.05 * (rng.random((lat.mask.size, 19)) - 0.5)))
+        inst.run(lbmb200.case(omega=1.2, xforce=3e-4, iterations=6))
+        got = np.array(inst.moments())
+        f = inst.get_field()[lat.mask != 0]
+    finally:
+        inst.deinit()
+    want = np.array([f.sum(), (f * CX).sum(), (f * CY).sum(), (f * CZ).sum()])
+    assert abs(got[0] - want[0]) / want[0] < 1e-12
+    scale = np.abs(f).sum()
+    assert np.all(np.abs(got[1:] - want[1:]) / scale < 1e-12)
