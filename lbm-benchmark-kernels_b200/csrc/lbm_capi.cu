@@ -697,14 +697,15 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* sla
         }
       g->listSlab = true;
     }
-    int* dMask = nullptr;
-    uint32_t* dGrid = nullptr;
-    LBM_CK(cudaMalloc(&dMask, sizeof(int) * ncell));
-    LBM_CK(cudaMalloc(&dGrid, sizeof(uint32_t) * ncell));
-    LBM_CK(cudaMemcpy(dMask, ld->Lattice, sizeof(int) * ncell, cudaMemcpyHostToDevice));
-    const int per3[3] = {ld->PeriodicX, ld->PeriodicY, ld->PeriodicZ};
-    const char* berr = "";
     if (!g->listSlab) {
+      // a slab's layout came from the host builder above
+      int* dMask = nullptr;
+      uint32_t* dGrid = nullptr;
+      LBM_CK(cudaMalloc(&dMask, sizeof(int) * ncell));
+      LBM_CK(cudaMalloc(&dGrid, sizeof(uint32_t) * ncell));
+      LBM_CK(cudaMemcpy(dMask, ld->Lattice, sizeof(int) * ncell, cudaMemcpyHostToDevice));
+      const int per3[3] = {ld->PeriodicX, ld->PeriodicY, ld->PeriodicZ};
+      const char* berr = "";
       const long long nf = lbm::list_build_device(dMask, ld->Dims, per3, pull ? 1 : 0, a.blk, nCells, dGrid, g->dAdj,
                                                   nTiles * lbm::kListTile, g->stream, &berr);
       if (nf != g->nFluid) {
@@ -712,9 +713,9 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* sla
         std::exit(1);
       }
       LBM_CK(cudaMemcpy(g->grid, dGrid, sizeof(uint32_t) * ncell, cudaMemcpyDeviceToHost));
+      LBM_CK(cudaFree(dGrid));
+      LBM_CK(cudaFree(dMask));
     }
-    LBM_CK(cudaFree(dGrid));
-    LBM_CK(cudaFree(dMask));
     {
       // the adjacency-driven steps read the run-compressed form (the full
       // adjacency stays for the host layout queries)

@@ -115,3 +115,20 @@ def test_reduced_storage_layout_pads_to_tiles():
         lo, hi = sl.halo_flags(r, 3, True)
         lay = sl.list_slab_layout(lat, x0, x1, lo, hi, ("-precision", "fp16"))
         assert lay["n_cells"] % 1024 == 0 and lay["n_cells"] >= lay["n_owned"] + lay["n_ghost"]
+
+
+def test_transport_word_counts():
+    """Messages of 2-, 4- and 8-byte PDF elements travel in whole 8-byte
+    words; both sides of a face compute the same word count."""
+    class S:
+        def __init__(self, eb, n):
+            self.elem_bytes, self.n = eb, n
+
+        def message(self, side, phase, send):
+            return self.n
+
+    assert sl.message(S(8, 5), 0, 0, True) == 5
+    assert sl.message(S(4, 5), 0, 0, True) == 3
+    assert sl.message(S(2, 5), 0, 0, True) == 2
+    assert sl.message(S(2, 8), 0, 0, True) == 2
+    assert sl.message(S(2, -1), 0, 0, True) == -1
