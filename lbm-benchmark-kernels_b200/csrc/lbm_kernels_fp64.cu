@@ -477,7 +477,7 @@ __global__ void __launch_bounds__(kListTile, 4) k_list_even_fp64(const ListArgs 
 // each of the 18 links, the 256 slots from the link of the tile's first node
 // on (consecutive nodes mostly reach consecutive slots), and the tile's own
 // rest-direction slots; one lane per region, clamped to the PDF array. The
-// tile's run record was prefetched into L2 one resident wave earlier.
+// tile's run record was prefetched into L2 half a resident wave earlier.
 __device__ __forceinline__ void prefetch_tile_pdfs(const ListArgs& a, unsigned u, int lane) {
   if (lane >= Q) return;
   const unsigned long long first =
@@ -496,15 +496,17 @@ __device__ __forceinline__ void prefetch_tile_pdfs(const ListArgs& a, unsigned u
 // packing 0.49 rows per node, 35 instead of 72 bytes per node. The block's
 // gathers are latency-bound at this occupancy (80 registers; a 64-register
 // build spills and is slower), so warp 2 prefetches into L2 the PDF regions
-// of the tile one resident wave ahead (records two waves ahead): 0.395 ->
-// 0.390 ms at the 256^3 packing.
+// of the tile half a resident wave ahead (the run records are one wave
+// ahead): 0.395 -> 0.371 ms at the 256^3 packing. Measured distances: one
+// wave 0.386 ms, two waves 0.435, a quarter wave 0.377.
 __global__ void __launch_bounds__(kListTile, 3) k_list_odd_fp64(const ListArgs a, const Trt<double> t) {
   __shared__ alignas(128) uint32_t srun[kRunTileWords];
   __shared__ alignas(8) uint64_t bar;
   __shared__ int ok;
-  if (!stage_run_tile<2>(a, srun, &bar, &ok)) return;
-  if (threadIdx.x >= 64 && threadIdx.x < 96 && a.prefetch > 0 && blockIdx.x + (unsigned)a.prefetch < gridDim.x)
-    prefetch_tile_pdfs(a, blockIdx.x + a.prefetch, threadIdx.x - 64);
+  if (!stage_run_tile(a, srun, &bar, &ok)) return;
+  const unsigned pdfAhead = static_cast<unsigned>(a.prefetch) / 2;
+  if (threadIdx.x >= 64 && threadIdx.x < 96 && pdfAhead > 0 && blockIdx.x + pdfAhead < gridDim.x)
+    prefetch_tile_pdfs(a, blockIdx.x + pdfAhead, threadIdx.x - 64);
   const int n = blockIdx.x * kListTile + threadIdx.x;
   if (n >= a.nFluid) return;
   uint32_t off;
