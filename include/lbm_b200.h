@@ -313,9 +313,21 @@ int lbm_aa_halo_pack(KernelData *kd, int side, int phase, void *buf, void *strea
 int lbm_aa_halo_unpack(KernelData *kd, int side, int phase, const void *buf, void *stream);
 int lbm_aa_slab_step(KernelData *kd, CaseData *cd, int half, void *stream);
 
+/* The odd step of a slab (lbm_aa_slab_step half 1) in two parts, so that the
+ * phase-0 messages can travel while part 0 runs: part 0 updates the cells
+ * whose odd step touches no halo slot (full-array slabs: the interior blocks;
+ * list slabs: the inner tile range, see lbm_aa_list_slab_layout) and needs no
+ * message; part 1 updates the rest and must follow the phase-0 unpack. Call
+ * each part once per pair; the phase-1 pack follows part 1. Together they
+ * equal lbm_aa_slab_step(half 1). Returns 0 or an error code. */
+int lbm_aa_slab_odd_part(KernelData *kd, CaseData *cd, int part, void *stream);
+
 /* The layout lbm_aa_list_slab_init builds, on the host only (no CUDA call):
- * counts[0..6] = owned nodes, ghost nodes, nCells, then the lengths of the
- * own / ghost slot lists of side 0 and of side 1 (-1: no halo). Non-NULL
+ * counts[0..8] = owned nodes, ghost nodes, nCells, then the lengths of the
+ * own / ghost slot lists of side 0 and of side 1 (-1: no halo), then the
+ * inner tile range [counts[7], counts[8]) of 256-node tiles whose nodes link
+ * to no ghost node (lbm_aa_slab_odd_part's part 0; empty when the face
+ * tiles are not all at the two ends of the numbering). Non-NULL
  * arrays receive the slab's numbering (x1-x0 by nY by nZ cells, x fastest;
  * obstacles 0xffffffff), the adjacency (owned nodes x 18, indices into
  * f[d * nCells + node]) and the four slot lists: own = the owned slots the

@@ -57,7 +57,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return false;
 }
 
-// Stages the run record of tile blockIdx.x (run-compressed adjacency, see
+// Stages the run record of tile blockIdx.x + a.tileBase (run-compressed adjacency, see
 // kRunHdrWords) into srun (kRunTileWords words) with one bulk copy. A record
 // whose size does not fit flags error bit 4 and is not copied. After the
 // wait, warp 1 prefetches into L2 the record of the tile kWaves x
@@ -67,8 +67,10 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // returns the same.
 template <int kWaves = 1, class A>
 __device__ __forceinline__ bool stage_run_tile(const A& a, uint32_t* srun, uint64_t* bar, int* ok) {
+  const unsigned tile = blockIdx.x + static_cast<unsigned>(a.tileBase);
+  const unsigned nTiles = static_cast<unsigned>((a.nFluid + kListTile - 1) / kListTile);
   if (threadIdx.x == 0) {
-    const uint32_t o0 = a.runOff[blockIdx.x], o1 = a.runOff[blockIdx.x + 1];
+    const uint32_t o0 = a.runOff[tile], o1 = a.runOff[tile + 1];
     const uint32_t bytes = (o1 - o0) * 16u;
     *ok = o1 > o0 && bytes <= static_cast<uint32_t>(kRunTileWords) * 4u;
     mbar_init(bar, 1);
@@ -85,8 +87,8 @@ __device__ __forceinline__ bool stage_run_tile(const A& a, uint32_t* srun, uint6
     if (threadIdx.x == 0) atomicOr(a.err, 1);
     return false;
   }
-  if (threadIdx.x == 32 && a.prefetch > 0 && blockIdx.x + kWaves * static_cast<unsigned>(a.prefetch) < gridDim.x) {
-    const unsigned t = blockIdx.x + kWaves * a.prefetch;
+  if (threadIdx.x == 32 && a.prefetch > 0 && tile + kWaves * static_cast<unsigned>(a.prefetch) < nTiles) {
+    const unsigned t = tile + kWaves * a.prefetch;
     const uint32_t o0 = a.runOff[t], o1 = a.runOff[t + 1];
     if (o1 > o0 && (o1 - o0) * 16u <= static_cast<uint32_t>(kRunTileWords) * 4u)
       bulk_prefetch_l2(a.runs + static_cast<size_t>(o0) * 4, (o1 - o0) * 16u);

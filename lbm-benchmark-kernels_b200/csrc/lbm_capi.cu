@@ -79,6 +79,7 @@ struct Gpu {
   uint32_t* dHalo[2][2];
   long long nHalo[2][2];
   bool listSlab;
+  int innerT0, innerT1;  // list slab: tiles whose odd step touches no halo slot
 
   // list layout
   uint32_t* grid;
@@ -319,6 +320,7 @@ lbm::ListArgs list_args(Gpu* g) {
   a.adj = g->dAdj;
   a.runs = g->dRuns;
   a.runOff = g->dRunOff;
+  a.tileBase = 0;
   a.nCells = g->nCells;
   a.nFluid = g->nFluid;
   a.err = g->dErr;
@@ -332,6 +334,7 @@ lbm::ListArgsLp list_args_lp(Gpu* g) {
   a.adj = g->dAdj;
   a.runs = g->dRuns;
   a.runOff = g->dRunOff;
+  a.tileBase = 0;
   a.nCells = g->nCells;
   a.nFluid = g->nFluid;
   a.err = g->dErr;
@@ -696,6 +699,7 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* sla
           }
         }
       g->listSlab = true;
+      lbmh_list_slab_inner_tiles(ls, lbm::kListTile, &g->innerT0, &g->innerT1);
     }
     if (!g->listSlab) {
       // a slab's layout came from the host builder above
@@ -1081,6 +1085,10 @@ int lbm_aa_list_slab_layout(const LatticeDesc* global, int x0, int x1, int haloL
   counts[4] = ls.ghost[0] ? ls.nGhostSlots[0] : -1;
   counts[5] = ls.own[1] ? ls.nOwnSlots[1] : -1;
   counts[6] = ls.ghost[1] ? ls.nGhostSlots[1] : -1;
+  int t0 = 0, t1 = 0;
+  lbmh_list_slab_inner_tiles(&ls, lbm::kListTile, &t0, &t1);
+  counts[7] = t0;
+  counts[8] = t1;
   const size_t cells = (size_t)ls.L * global->Dims[1] * global->Dims[2];
   if (grid) std::memcpy(grid, ls.grid, sizeof(uint32_t) * cells);
   if (adj && ls.nOwned > 0) std::memcpy(adj, ls.adj, sizeof(uint32_t) * QM * (size_t)ls.nOwned);
@@ -1206,6 +1214,51 @@ int lbm_aa_slab_step(KernelData* kd, CaseData* cd, int half, void* stream) {
     if (lbm::aa_shell_cells(a) > 0) lbm::aa_odd_face_fp64(a, t, s);
     g->iteration += 2;
   }
+  return (int)cudaGetLastError();
+}
+
+int lbm_aa_slab_odd_part(KernelData* kd, CaseData* cd, int part, void* stream) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (part < 0 || part > 1 || (g->kind != kAa && !g->listSlab)) return -1;
+  sync_upload(g);
+  const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
+  const cudaStream_t s = stream_or(g, stream);
+  if (g->listSlab) {
+    const int nTiles = (g->nFluid + lbm::kListTile - 1) / lbm::kListTile;
+    // part 0: the inner tiles; part 1: the tiles before and after them (all
+    // tiles when the slab has no inner range)
+    int r[2][2] = {{0, 0}, {0, 0}};
+    if (g->innerT1 > g->innerT0) {
+      if (part == 0) {
+        r[0][0] = g->innerT0;
+        r[0][1] = g->innerT1;
+      } else {
+        r[0][1] = g->innerT0;
+        r[1][0] = g->innerT1;
+        r[1][1] = nTiles;
+      }
+    } else if (part == 1) {
+      r[0][1] = nTiles;
+    }
+    for (int k = 0; k < 2; ++k) {
+      const int t0 = r[k][0], t1 = r[k][1];
+      if (t1 <= t0) continue;
+      if (g->storage != lbm::kStoreF64)
+        lbm::list_odd_lp_tiles(list_args_lp(g), to_float(t), g->storage, t0, t1, s);
+      else
+        lbm::list_odd_fp64_tiles(list_args(g), t, t0, t1, s);
+    }
+  } else {
+    const lbm::AaArgs a = aa_args(g);
+    if (part == 0) {
+      // the interior blocks read and write only the slab's own planes
+      if (g->nDirect > 0) lbm::aa_odd_interior_fp64(a, t, g->dOddBlocks, g->nDirect, 0, s);
+      if (g->nGeneral > 0) lbm::aa_odd_interior_fp64(a, t, g->dOddBlocks + g->nDirect, 0, g->nGeneral, s);
+    } else if (lbm::aa_shell_cells(a) > 0) {
+      lbm::aa_odd_face_fp64(a, t, s);
+    }
+  }
+  if (part == 1) g->iteration += 2;
   return (int)cudaGetLastError();
 }
 

@@ -409,6 +409,26 @@ done:
 	return rc;
 }
 
+void lbmh_list_slab_inner_tiles(const LbmhListSlab *s, int tile, int *t0, int *t1)
+{
+	const int nOwned = s->nOwned;
+	const int nTiles = (nOwned + tile - 1) / tile;
+	/* a tile is inner when none of its nodes links to a ghost node */
+	int lead = 0, trail = 0, inner = 1;
+	char *face = (char *)calloc(nTiles > 0 ? nTiles : 1, 1);
+	if (!face) { *t0 = *t1 = 0; return; }
+	for (long n = 0; n < nOwned; ++n)
+		for (int d = 0; d < 18; ++d)
+			if ((int)(s->adj[n * 18 + d] % (uint32_t)s->nCells) >= nOwned) { face[n / tile] = 1; break; }
+	while (lead < nTiles && face[lead]) ++lead;
+	while (trail < nTiles - lead && face[nTiles - 1 - trail]) ++trail;
+	for (int t = lead; t < nTiles - trail; ++t) inner &= !face[t];
+	free(face);
+	if (!inner || lead >= nTiles - trail) { *t0 = *t1 = 0; return; }
+	*t0 = lead;
+	*t1 = nTiles - trail;
+}
+
 /* ------------------------------------------------------------------------ */
 /* AA link words. A link d of fluid cell x is "reversed" when x + c_d is not a
  * fluid node reached directly or through a periodic wrap: an obstacle inside

@@ -61,6 +61,14 @@ int lbmh_list_slab_build(const LatticeDesc *ld, int x0, int x1, const int halo[2
                          const char *pad, int quantum, LbmhListSlab *s);
 void lbmh_list_slab_free(LbmhListSlab *s);
 
+/* The slab's inner tiles (of `tile` owned nodes): [*t0, *t1), a contiguous
+ * range of tiles none of whose nodes links to a ghost node, so that their
+ * odd step reads and writes no halo slot. With the default numbering the
+ * slab's two face planes are its first and last nodes and the range is the
+ * rest; when face tiles are not all at the ends (blocked numbering), or
+ * nothing is inner, the range is empty (0, 0). */
+void lbmh_list_slab_inner_tiles(const LbmhListSlab *s, int tile, int *t0, int *t1);
+
 /* Link words of the full-array AA layout: for every cell of the padded
  * (nX+2) x (nY+2) x pitch array, bit 31 = fluid cell, bit d = link d of the
  * cell does not reach a fluid node (wall or open face). Ghost and pad cells

@@ -91,6 +91,7 @@ struct ListArgs {
   int prefetch;   // tiles ahead whose adjacency a block prefetches into L2 (0: none)
   const uint32_t* runs;    // run-compressed adjacency (list AA odd step, list push)
   const uint32_t* runOff;  // nTiles + 1 tile offsets into runs, 16-byte units
+  int tileBase;            // first tile of the launch (block b updates tile tileBase + b)
 };
 
 // The prefetch distance of a launch of `kernel` (threads per block): its
@@ -132,6 +133,7 @@ struct ListArgsLp {
   int nFluid;
   int* err;
   int prefetch;  // as ListArgs::prefetch
+  int tileBase;  // as ListArgs::tileBase
 };
 
 // List layout built on the device (lbm_build.cu): numbering into grid (one
@@ -157,6 +159,10 @@ int list_runs_device(const uint32_t* adj, int nFluid, cudaStream_t s, uint32_t**
 // Launchers (stream-ordered, no synchronisation).
 void list_even_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s);
 void list_odd_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s);
+// The odd steps over tiles [t0, t1) only (slabs overlap their halo exchange
+// with the tiles that read no ghost node).
+void list_odd_fp64_tiles(const ListArgs& a, const Trt<double>& t, int t0, int t1, cudaStream_t s);
+void list_odd_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int storage, int t0, int t1, cudaStream_t s);
 void aa_even_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
 // The AA odd step: the interior blocks (a list of nDirect blocks for the
 // direct kernel, followed by nGeneral blocks for the general one, built by

@@ -465,7 +465,7 @@ void aa_odd_face_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
 
 // 4 blocks of 256 threads per SM (64 registers, no spills)
 __global__ void __launch_bounds__(kListTile, 4) k_list_even_fp64(const ListArgs a, const Trt<double> t) {
-  const int n = blockIdx.x * kListTile + threadIdx.x;
+  const int n = blockIdx.x * kListTile + threadIdx.x;  // the even step is never split
   if (n >= a.nFluid) return;
   double* const f = a.f + n;
   double* const fs = launder(f);
@@ -504,10 +504,12 @@ __global__ void __launch_bounds__(kListTile, 3) k_list_odd_fp64(const ListArgs a
   __shared__ alignas(8) uint64_t bar;
   __shared__ int ok;
   if (!stage_run_tile(a, srun, &bar, &ok)) return;
+  const unsigned tile = blockIdx.x + static_cast<unsigned>(a.tileBase);
   const unsigned pdfAhead = static_cast<unsigned>(a.prefetch) / 2;
-  if (threadIdx.x >= 64 && threadIdx.x < 96 && pdfAhead > 0 && blockIdx.x + pdfAhead < gridDim.x)
-    prefetch_tile_pdfs(a, blockIdx.x + pdfAhead, threadIdx.x - 64);
-  const int n = blockIdx.x * kListTile + threadIdx.x;
+  if (threadIdx.x >= 64 && threadIdx.x < 96 && pdfAhead > 0 &&
+      tile + pdfAhead < static_cast<unsigned>((a.nFluid + kListTile - 1) / kListTile))
+    prefetch_tile_pdfs(a, tile + pdfAhead, threadIdx.x - 64);
+  const int n = static_cast<int>(tile) * kListTile + threadIdx.x;
   if (n >= a.nFluid) return;
   uint32_t off;
   const uint32_t* e = run_row(srun, threadIdx.x, off);  // link d = e[d] + off
@@ -537,7 +539,7 @@ __global__ void __launch_bounds__(kListTile) k_list_pull_fp64(const ListArgs a, 
   __shared__ alignas(8) uint64_t bar;
   __shared__ int ok;
   if (!stage_run_tile(a, srun, &bar, &ok)) return;
-  const int n = blockIdx.x * kListTile + threadIdx.x;
+  const int n = (blockIdx.x + a.tileBase) * kListTile + threadIdx.x;
   if (n >= a.nFluid) return;
   uint32_t off;
   const uint32_t* e = run_row(srun, threadIdx.x, off);  // link d = e[d] + off (run-compressed pull adjacency)
@@ -563,7 +565,7 @@ __global__ void __launch_bounds__(kListTile, 3) k_list_push_fp64(const ListArgs 
   __shared__ alignas(8) uint64_t bar;
   __shared__ int ok;
   if (!stage_run_tile(a, srun, &bar, &ok)) return;
-  const int n = blockIdx.x * kListTile + threadIdx.x;
+  const int n = (blockIdx.x + a.tileBase) * kListTile + threadIdx.x;
   if (n >= a.nFluid) return;
   uint32_t off;
   const uint32_t* e = run_row(srun, threadIdx.x, off);
@@ -627,12 +629,22 @@ static unsigned list_blocks(const ListArgs& a) { return (a.nFluid + kListTile - 
 void list_even_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s) {
   if (a.nFluid > 0) k_list_even_fp64<<<list_blocks(a), kListTile, 0, s>>>(a, t);
 }
+static std::atomic<int> g_oddAhead{0};
+
 void list_odd_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s) {
-  static std::atomic<int> ahead{0};
   if (a.nFluid <= 0) return;
   ListArgs b = a;
-  b.prefetch = prefetch_distance(ahead, k_list_odd_fp64, kListTile, a.prefetch != 0);
+  b.tileBase = 0;
+  b.prefetch = prefetch_distance(g_oddAhead, k_list_odd_fp64, kListTile, a.prefetch != 0);
   k_list_odd_fp64<<<list_blocks(b), kListTile, 0, s>>>(b, t);
+}
+
+void list_odd_fp64_tiles(const ListArgs& a, const Trt<double>& t, int t0, int t1, cudaStream_t s) {
+  if (a.nFluid <= 0 || t1 <= t0) return;
+  ListArgs b = a;
+  b.tileBase = t0;
+  b.prefetch = prefetch_distance(g_oddAhead, k_list_odd_fp64, kListTile, a.prefetch != 0);
+  k_list_odd_fp64<<<(unsigned)(t1 - t0), kListTile, 0, s>>>(b, t);
 }
 void list_pull_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s) {
   // no adjacency prefetch: with the full adjacency it slowed this kernel by

@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(kListTile) k_list_odd_lp(const ListArgsLp a, c
   __shared__ alignas(8) uint64_t bar;
   __shared__ int ok;
   if (!stage_run_tile(a, srun, &bar, &ok)) return;
-  const int n = blockIdx.x * kListTile + threadIdx.x;
+  const int n = (blockIdx.x + a.tileBase) * kListTile + threadIdx.x;
   if (n >= a.nFluid) return;
   uint32_t off;
   const uint32_t* e = run_row(srun, threadIdx.x, off);  // link d = e[d] + off (run-compressed adjacency)
@@ -181,10 +181,25 @@ void list_even_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStr
     k_list_even_lp<StoreF32><<<lp_blocks(a), kListTile, 0, s>>>(a, t);
 }
 
+static std::atomic<int> ahead16{0}, ahead32{0};
+
+void list_odd_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int storage, int t0, int t1, cudaStream_t s) {
+  if (a.nFluid <= 0 || t1 <= t0) return;
+  ListArgsLp b = a;
+  b.tileBase = t0;
+  if (storage == kStoreF16) {
+    b.prefetch = prefetch_distance(ahead16, k_list_odd_lp<StoreF16>, kListTile, a.prefetch != 0);
+    k_list_odd_lp<StoreF16><<<(unsigned)(t1 - t0), kListTile, 0, s>>>(b, t);
+  } else {
+    b.prefetch = prefetch_distance(ahead32, k_list_odd_lp<StoreF32>, kListTile, a.prefetch != 0);
+    k_list_odd_lp<StoreF32><<<(unsigned)(t1 - t0), kListTile, 0, s>>>(b, t);
+  }
+}
+
 void list_odd_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s) {
   if (a.nFluid <= 0) return;
-  static std::atomic<int> ahead16{0}, ahead32{0};
   ListArgsLp b = a;
+  b.tileBase = 0;
   if (storage == kStoreF16) {
     b.prefetch = prefetch_distance(ahead16, k_list_odd_lp<StoreF16>, kListTile, a.prefetch != 0);
     k_list_odd_lp<StoreF16><<<lp_blocks(b), kListTile, 0, s>>>(b, t);

@@ -33,6 +33,8 @@ def main(argv=None):
     p.add_argument("--layout", default="full", choices=("full", "list"))
     p.add_argument("--precision", default="fp64", choices=("fp64", "fp32", "fp16"),
                    help="PDF storage of list slabs")
+    p.add_argument("--overlap", action="store_true",
+                   help="send the phase-0 halo messages while the inner cells take their odd step")
     a = p.parse_args(argv)
 
     import torch
@@ -66,18 +68,18 @@ def main(argv=None):
         tr = sl.DistTransport(slab, ranks.rank, ranks.world, ring, dist,
                               lambda n: torch.empty(n, dtype=torch.float64, device="cuda"), stream=stream)
         cd = lbmb200.case(omega=a.omega, xforce=1e-5)
-        sl.step_pairs([slab], tr, cd, a.warmup, stream)
+        sl.step_pairs([slab], tr, cd, a.warmup, stream, overlap=a.overlap)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         ranks.barrier()
         e0.record()
-        sl.step_pairs([slab], tr, cd, a.pairs, stream)
+        sl.step_pairs([slab], tr, cd, a.pairs, stream, overlap=a.overlap)
         e1.record()
         torch.cuda.synchronize()
         ms = ranks.max(e0.elapsed_time(e1))
         nodes = ranks.sum(slab.local.n_fluid)
         rec = {"dims": dims, "geometry": a.geometry, "layout": a.layout, "precision": a.precision,
-               "ranks": ranks.world,
+               "overlap": a.overlap, "ranks": ranks.world,
                "fluid_nodes": nodes, "pairs": a.pairs, "ms": round(ms, 3),
                "mflups": round(nodes * 2 * a.pairs / (ms / 1e3) / 1e6, 1)}
         if a.layout == "list":

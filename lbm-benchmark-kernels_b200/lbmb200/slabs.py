@@ -84,6 +84,8 @@ def _sigs(L):
             getattr(L, name).argtypes = [ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                          ctypes.c_void_p]
         L.lbm_aa_slab_step.argtypes = [ctypes.POINTER(KernelData), ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.lbm_aa_slab_odd_part.argtypes = [ctypes.POINTER(KernelData), ctypes.c_void_p, ctypes.c_int,
+                                           ctypes.c_void_p]
         L._slab_sigs = True
     return L
 
@@ -135,6 +137,13 @@ class Slab:
         rc = self.L.lbm_aa_slab_step(self.kdp, ctypes.byref(cd), int(half), stream)
         if rc:
             raise RuntimeError("slab step failed (%d)" % rc)
+
+    def odd_part(self, cd, part, stream=None):
+        """Part 0 (cells that touch no halo slot) or part 1 (the rest) of the
+        odd step: lbm_aa_slab_odd_part."""
+        rc = self.L.lbm_aa_slab_odd_part(self.kdp, ctypes.byref(cd), int(part), stream)
+        if rc:
+            raise RuntimeError("slab odd step part failed (%d)" % rc)
 
     def pack(self, side, phase, buf, stream=None):
         rc = self.L.lbm_aa_halo_pack(self.kdp, int(side), int(phase), _ptr(buf), stream)
@@ -198,6 +207,14 @@ class LocalTransport:
             self.slabs[q].pack(0, phase, to_left, self.stream)
             self.slabs[r].unpack(1, phase, to_left, self.stream)
 
+    # all slabs share one stream, so a started exchange is already complete
+    # in stream order
+    def start(self, phase):
+        self.exchange(phase)
+
+    def finish(self, phase):
+        pass
+
 
 class DistTransport:
     """One slab per rank: paired isend/irecv with the left and right
@@ -211,12 +228,20 @@ class DistTransport:
         # one buffer per face and direction; each phase's message is a prefix
         self.send = {s: make_buf(max(1, max(message(slab, s, p, True) for p in (0, 1)))) for s in (0, 1)}
         self.recv = {s: make_buf(max(1, max(message(slab, s, p, False) for p in (0, 1)))) for s in (0, 1)}
+        self._reqs, self._inc = [], {}
 
     def exchange(self, phase, sync=None):
+        self.start(phase, sync)
+        self.finish(phase)
+
+    def start(self, phase, sync=None):
+        """Packs this slab's messages and posts the sends and receives; they
+        travel while the caller enqueues more work (with NCCL the library's
+        stream waits for the packs, then runs beside the caller's stream)."""
         d = self.dist
         faces = [s for s in (1, 0) if (self.right if s else self.left) is not None]
         out = {s: self.send[s][:message(self.slab, s, phase, True)] for s in faces}
-        inc = {s: self.recv[s][:message(self.slab, s, phase, False)] for s in faces}
+        self._inc = {s: self.recv[s][:message(self.slab, s, phase, False)] for s in faces}
         for side in faces:
             self.slab.pack(side, phase, out[side], self.stream)
         if sync:
@@ -227,23 +252,29 @@ class DistTransport:
                 ops.append(d.P2POp(d.isend, out[side], peer))
         for side, peer in ((0, self.left), (1, self.right)):
             if peer is not None:
-                ops.append(d.P2POp(d.irecv, inc[side], peer))
-        if ops:
-            for req in d.batch_isend_irecv(ops):
-                req.wait()
+                ops.append(d.P2POp(d.irecv, self._inc[side], peer))
+        self._reqs = d.batch_isend_irecv(ops) if ops else []
+
+    def finish(self, phase):
+        """Waits for the posted messages (on NCCL: the caller's stream waits)
+        and unpacks the received ones."""
+        for req in self._reqs:
+            req.wait()
+        self._reqs = []
         for side in (0, 1):
             if (self.right if side else self.left) is not None:
-                self.slab.unpack(side, phase, inc[side], self.stream)
+                self.slab.unpack(side, phase, self._inc[side], self.stream)
 
 
 def list_slab_layout(lattice, x0, x1, halo_lo, halo_hi, kernel_args=()):
     """The layout of a list slab, built on the host (no CUDA call): a dict
     with n_owned, n_ghost, n_cells, grid (slab cells, x fastest), adj
-    (n_owned x 18) and the slot lists own / ghost per side (None: no halo)."""
+    (n_owned x 18), the slot lists own / ghost per side (None: no halo) and
+    the inner tile range (256-node tiles that link to no ghost node)."""
     L = _sigs(lib())
     nx, ny, nz = lattice.dims
     p, argv = _params(kernel_args)
-    counts = (ctypes.c_longlong * 7)()
+    counts = (ctypes.c_longlong * 9)()
     args = (ctypes.byref(lattice.desc), x0, x1, int(halo_lo), int(halo_hi), ctypes.byref(p), counts)
     rc = L.lbm_aa_list_slab_layout(*args, None, None, None, None, None, None)
     if rc:
@@ -258,17 +289,28 @@ def list_slab_layout(lattice, x0, x1, halo_lo, halo_hi, kernel_args=()):
         raise RuntimeError("list slab layout failed (%d)" % rc)
     cut = [lists[k][:counts[3 + k]] if counts[3 + k] >= 0 else None for k in range(4)]
     return {"n_owned": n_owned, "n_ghost": counts[1], "n_cells": counts[2], "grid": grid,
-            "adj": adj[: n_owned * 18], "own": (cut[0], cut[2]), "ghost": (cut[1], cut[3])}
+            "adj": adj[: n_owned * 18], "own": (cut[0], cut[2]), "ghost": (cut[1], cut[3]),
+            "inner": (counts[7], counts[8])}
 
 
-def step_pairs(slabs, transport, cd, pairs, stream=None):
-    """`pairs` even/odd step pairs of a slab-decomposed lattice."""
+def step_pairs(slabs, transport, cd, pairs, stream=None, overlap=False):
+    """`pairs` even/odd step pairs of a slab-decomposed lattice. With
+    `overlap`, the phase-0 messages travel while the cells that need no halo
+    data take their odd step (Slab.odd_part 0); the rest follows the unpack."""
     for _ in range(pairs):
         for s in slabs:
             s.step(cd, 0, stream)
-        transport.exchange(0)
-        for s in slabs:
-            s.step(cd, 1, stream)
+        if overlap:
+            transport.start(0)
+            for s in slabs:
+                s.odd_part(cd, 0, stream)
+            transport.finish(0)
+            for s in slabs:
+                s.odd_part(cd, 1, stream)
+        else:
+            transport.exchange(0)
+            for s in slabs:
+                s.step(cd, 1, stream)
         transport.exchange(1)
 
 

@@ -590,11 +590,18 @@ static void list_odd(orc_state_t *s, const trt_t *t)
 int orc_list_aa_half(int odd, int n_nodes, int n_cells, const uint32_t *adj, double *f,
                      double omega, double lambda, double xforce)
 {
+	return orc_list_aa_half_range(odd, 0, n_nodes, n_cells, adj, f, omega, lambda, xforce);
+}
+
+/* The same over nodes [n0, n1) only (adj indexed by node: adj[n * 18]). */
+int orc_list_aa_half_range(int odd, int n0, int n1, int n_cells, const uint32_t *adj, double *f,
+                           double omega, double lambda, double xforce)
+{
 	const trt_t t = trt_make(omega, lambda);
 	double ft[Q];
 	for (int d = 0; d < Q; ++d) ft[d] = force_term(d, xforce);
 	const size_t nc = (size_t)n_cells;
-	for (int n = 0; n < n_nodes; ++n) {
+	for (int n = n0; n < n1; ++n) {
 		double p[Q], o[Q];
 		if (!odd) {
 			for (int d = 0; d < Q; ++d) p[d] = f[d * nc + n];

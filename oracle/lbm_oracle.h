@@ -74,6 +74,9 @@ int orc_run(int kernel, const int dims[3], const int periodic[3], const int *lat
  * owned ones. */
 int orc_list_aa_half(int odd, int n_nodes, int n_cells, const uint32_t *adj, double *f,
                      double omega, double lambda, double xforce);
+/* The same half step over nodes [n0, n1) only (adj indexed by node). */
+int orc_list_aa_half_range(int odd, int n0, int n1, int n_cells, const uint32_t *adj, double *f,
+                           double omega, double lambda, double xforce);
 
 /* The reference's -verify check (src/Kernel.c:451-625) on a field of logical
  * PDFs (same layout as orc_run's out_pdfs). Returns the L2 norm of the

@@ -101,6 +101,15 @@ class Oracle:
                                        ctypes.c_double(xforce))
         assert rc == 0
 
+    def list_aa_half_range(self, odd, n0, n1, n_cells, adj, f, omega=1.0, lam=1.0 / 12.0, xforce=1e-5):
+        """list_aa_half over nodes [n0, n1) only: orc_list_aa_half_range."""
+        assert f.dtype == np.float64 and f.flags.c_contiguous and f.size >= 19 * n_cells
+        adj = np.ascontiguousarray(adj, dtype=np.uint32)
+        rc = self.lib.orc_list_aa_half_range(int(odd), int(n0), int(n1), int(n_cells), _p(adj, ctypes.c_uint32),
+                                             _p(f, ctypes.c_double), ctypes.c_double(omega), ctypes.c_double(lam),
+                                             ctypes.c_double(xforce))
+        assert rc == 0
+
     def verify_error(self, dims, lat, pdfs, omega=1.0, xforce=1e-5):
         pdfs = np.ascontiguousarray(pdfs, dtype=np.float64).reshape(-1)
         return self.lib.orc_verify_error(_i3(*dims), _p(lat, ctypes.c_int), _p(pdfs, ctypes.c_double),

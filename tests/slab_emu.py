@@ -45,6 +45,19 @@ class EmuSlab:
     def half(self, oracle, odd):
         oracle.list_aa_half(odd, self.lay["n_owned"], self.nc, self.lay["adj"], self.f, OMEGA, LAM, XF)
 
+    def odd_part(self, oracle, part):
+        """Part 0 (the inner tiles, no ghost links) or part 1 (the rest) of
+        the odd step, by the library's inner tile range."""
+        t0, t1 = self.lay["inner"]
+        no = self.lay["n_owned"]
+        if t1 > t0:
+            ranges = [(t0 * 256, min(t1 * 256, no))] if part == 0 else [(0, t0 * 256), (min(t1 * 256, no), no)]
+        else:
+            ranges = [] if part == 0 else [(0, no)]
+        for n0, n1 in ranges:
+            if n1 > n0:
+                oracle.list_aa_half_range(1, n0, n1, self.nc, self.lay["adj"], self.f, OMEGA, LAM, XF)
+
     def idx(self, side, phase, pack):
         own = (phase == 0) == pack
         return (self.lay["own"] if own else self.lay["ghost"])[side]
@@ -71,9 +84,11 @@ def exchange(slabs, faces, phase):
         a.f[a.idx(1, phase, False)] = b.f[b.idx(0, phase, True)]
 
 
-def run_slabs(oracle, lat, parts, pairs, init, kargs=()):
+def run_slabs(oracle, lat, parts, pairs, init, kargs=(), overlap=False):
     """`pairs` step pairs of `lat` split into `parts` slabs in this process;
-    returns the gathered logical field and the slabs."""
+    returns the gathered logical field and the slabs. With `overlap`, the
+    phase-0 messages are packed, then the inner tiles take their odd step,
+    then the messages are unpacked and the other tiles follow."""
     nx = lat.dims[0]
     ring = sl.is_ring(lat.periodic)
     slabs = []
@@ -90,9 +105,20 @@ def run_slabs(oracle, lat, parts, pairs, init, kargs=()):
     for _ in range(pairs):
         for s in slabs:
             s.half(oracle, 0)
-        exchange(slabs, faces, 0)
-        for s in slabs:
-            s.half(oracle, 1)
+        if overlap:
+            sent = [(a.f[a.idx(1, 0, True)].copy(), b.f[b.idx(0, 0, True)].copy())
+                    for a, b in ((slabs[r], slabs[q]) for r, q in faces)]
+            for s in slabs:
+                s.odd_part(oracle, 0)
+            for (r, q), (to_right, to_left) in zip(faces, sent):
+                slabs[q].f[slabs[q].idx(0, 0, False)] = to_right
+                slabs[r].f[slabs[r].idx(1, 0, False)] = to_left
+            for s in slabs:
+                s.odd_part(oracle, 1)
+        else:
+            exchange(slabs, faces, 0)
+            for s in slabs:
+                s.half(oracle, 1)
         exchange(slabs, faces, 1)
     out = np.zeros_like(init)
     for s in slabs:

@@ -28,7 +28,7 @@ CASES = [
 ]
 
 
-def _run_slabs(lat, parts, init, cd, pairs, layout="full", kargs=("-lambda", "3/16")):
+def _run_slabs(lat, parts, init, cd, pairs, layout="full", kargs=("-lambda", "3/16"), overlap=False):
     import torch
     work = torch.cuda.Stream()  # an explicit stream orders all slabs' operations
     stream = work.cuda_stream
@@ -40,7 +40,7 @@ def _run_slabs(lat, parts, init, cd, pairs, layout="full", kargs=("-lambda", "3/
         sl.scatter_field(slabs, lat, init)
         tr = sl.LocalTransport(slabs, ring, stream,
                                lambda n: torch.empty(n, dtype=torch.float64, device="cuda"))
-        sl.step_pairs(slabs, tr, cd, pairs, stream)
+        sl.step_pairs(slabs, tr, cd, pairs, stream, overlap=overlap)
         torch.cuda.synchronize()
         return sl.gather_field(slabs, lat)
     finally:
@@ -181,3 +181,30 @@ def test_slabrun_list_fp32_single_process(capsys):
     assert rec["precision"] == "fp32" and rec["mflups"] > 0
     assert abs(rec["sum_rho"] - rec["fluid_nodes"]) < 1e-6 * rec["fluid_nodes"]
     assert rec["sum_jx"] > 0 and rec["permeability"] > 0
+
+
+@pytest.mark.parametrize("layout,kargs,geo,dims,per,parts", [
+    ("full", ["-lambda", "3/16"], "fluid", (25, 9, 11), (1, 1, 1), 3),
+    ("full", ["-lambda", "3/16"], "channel", (30, 12, 14), (0, 0, 0), 3),
+    ("list", ["-lambda", "3/16", "-pad", "no"], "spheres", (30, 24, 24), (1, 1, 1), 3),
+    ("list", ["-lambda", "3/16", "-precision", "fp32"], "spheres", (30, 24, 24), (1, 1, 1), 2),
+    ("list", ["-lambda", "3/16", "-blk", "4"], "fluid", (16, 12, 12), (1, 1, 1), 2),  # no inner tile range
+])
+def test_overlapped_odd_step_equals_whole_lattice(layout, kargs, geo, dims, per, parts):
+    """The odd step in two parts around the phase-0 exchange
+    (lbm_aa_slab_odd_part) leaves the single instance's bits."""
+    lat = _lattice(geo, dims, per)
+    rng = np.random.default_rng(8)
+    init = lbmb200.W[None, :] * (1.0 + 0.05 * (rng.random((lat.mask.size, 19)) - 0.5))
+    cd = lbmb200.case(omega=1.1, xforce=2e-4, iterations=10)
+    kname = "cuda-aa-soa" if layout == "full" else "cuda-list-aa-pv-soa"
+    inst = lbmb200.kernel(kname).init(lat, kernel_args=kargs)
+    try:
+        inst.set_field(init)
+        inst.run(cd)
+        whole = inst.get_field()
+    finally:
+        inst.deinit()
+    got = _run_slabs(lat, parts, init, cd, 5, layout=layout, kargs=kargs, overlap=True)
+    m = lat.mask != 0
+    assert np.array_equal(got[m], whole[m])

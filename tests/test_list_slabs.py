@@ -132,3 +132,35 @@ def test_transport_word_counts():
     assert sl.message(S(2, 5), 0, 0, True) == 2
     assert sl.message(S(2, 8), 0, 0, True) == 2
     assert sl.message(S(2, -1), 0, 0, True) == -1
+
+
+@pytest.mark.parametrize("geo,dims,per,parts,kargs", [
+    ("channel", (24, 16, 16), (1, 1, 0), 3, ()),
+    ("fluid", (20, 12, 12), (1, 1, 1), 2, ("-pad", "no")),
+    ("box", (24, 12, 12), (0, 0, 0), 3, ("-pad", "no")),
+    ("fluid", (9, 5, 6), (0, 0, 1), 2, ("-blk", "2")),   # blocked numbering: no inner range
+])
+def test_overlapped_odd_step_matches_undivided_run(oracle, geo, dims, per, parts, kargs):
+    """The odd step split into the inner tiles (run while the phase-0 messages
+    travel) and the rest (after they arrive) leaves the same bits."""
+    lat = lbmb200.geometry(geo, dims, per)
+    init = _init_field(lat, 13)
+    want = oracle.run("list-aa", lat.dims, lat.periodic, lat.mask, omega=OMEGA, lam=LAM, xforce=XF,
+                      iterations=6, init="pdfs", init_pdfs=init)
+    got, slabs = run_slabs(oracle, lat, parts, 3, init, kargs, overlap=True)
+    fl = lat.mask != 0
+    assert np.array_equal(got[fl], want[fl])
+    if "-blk" not in kargs:
+        assert any(s.lay["inner"][1] > s.lay["inner"][0] for s in slabs)
+
+
+def test_inner_tiles_link_to_no_ghost():
+    lat, _ = lbmb200.spheres((24, 12, 12), 5, 0.5, 2.0, 3.0, 2000)
+    for r, (x0, x1) in enumerate(sl.partition(24, 2)):
+        lo, hi = sl.halo_flags(r, 2, True)
+        lay = sl.list_slab_layout(lat, x0, x1, lo, hi, ("-pad", "no"))
+        t0, t1 = lay["inner"]
+        assert 0 < t0 < t1
+        adj = lay["adj"].reshape(-1, 18)
+        inner = adj[t0 * 256: min(t1 * 256, lay["n_owned"])]
+        assert np.all(inner % lay["n_cells"] < lay["n_owned"])

@@ -96,10 +96,17 @@ LIST_SCRIPT = textwrap.dedent("""
     slab.set_field(init_field(lat, 5))
     tr = sl.DistTransport(slab, r.rank, r.world, ring, dist, lambda n: torch.zeros(n, dtype=torch.float64))
     orc = Oracle()
+    overlap = len(sys.argv) > 5 and sys.argv[5] == "1"
     for _ in range(pairs):
         slab.half(orc, 0)
-        tr.exchange(0)
-        slab.half(orc, 1)
+        if overlap:
+            tr.start(0)
+            slab.odd_part(orc, 0)
+            tr.finish(0)
+            slab.odd_part(orc, 1)
+        else:
+            tr.exchange(0)
+            slab.half(orc, 1)
         tr.exchange(1)
     out = np.zeros((lat.mask.size, 19))
     slab.get_field(out)
@@ -109,12 +116,17 @@ LIST_SCRIPT = textwrap.dedent("""
 """)
 
 
-@pytest.mark.parametrize("world,geo,dims,per", [(2, "fluid", "6x5x4", "111"), (3, "channel", "9x6x5", "110"),
-                                                 (2, "box", "8x5x5", "000")])
-def test_list_slabs_over_gloo_match_undivided_run(tmp_path, oracle, world, geo, dims, per):
+@pytest.mark.parametrize("world,geo,dims,per,overlap", [(2, "fluid", "6x5x4", "111", 0),
+                                                         (3, "channel", "9x6x5", "110", 0),
+                                                         (2, "box", "8x5x5", "000", 0),
+                                                         (2, "fluid", "20x12x12", "111", 1),
+                                                         (3, "channel", "24x16x16", "110", 1)])
+def test_list_slabs_over_gloo_match_undivided_run(tmp_path, oracle, world, geo, dims, per, overlap):
     """List-AA slabs as gloo ranks: the layout from the library, the steps
-    from the oracle, the halo messages through DistTransport; the gathered
-    field equals the undivided oracle run bit for bit."""
+    from the oracle, the halo messages through DistTransport (with `overlap`,
+    the phase-0 messages are posted, the inner tiles step, then the messages
+    are awaited and the other tiles step); the gathered field equals the
+    undivided oracle run bit for bit."""
     sys.path[:0] = [os.path.join(ROOT, "tests")]
     import numpy as np
     import lbmb200
@@ -123,8 +135,8 @@ def test_list_slabs_over_gloo_match_undivided_run(tmp_path, oracle, world, geo, 
     script.write_text(LIST_SCRIPT % {"root": ROOT, "out": str(tmp_path)})
     pairs = 3
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=%d" % world,
-           "--master-addr=127.0.0.1", "--master-port=%d" % (29571 + world + 7 * len(geo)), str(script),
-           geo, dims, per, str(pairs)]
+           "--master-addr=127.0.0.1", "--master-port=%d" % (29571 + world + 7 * len(geo) + 50 * overlap),
+           str(script), geo, dims, per, str(pairs), str(overlap)]
     out = subprocess.run(cmd, capture_output=True, text=True, timeout=240, env=dict(os.environ, OMP_NUM_THREADS="1"))
     assert out.returncode == 0, out.stderr[-3000:]
     d = tuple(int(v) for v in dims.split("x"))
