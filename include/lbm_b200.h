@@ -322,6 +322,15 @@ int lbm_aa_slab_step(KernelData *kd, CaseData *cd, int half, void *stream);
  * equal lbm_aa_slab_step(half 1). Returns 0 or an error code. */
 int lbm_aa_slab_odd_part(KernelData *kd, CaseData *cd, int part, void *stream);
 
+/* The even step (half 0) in the same two parts, so that the phase-1
+ * messages of the previous pair can travel while part 0 runs: part 0 updates
+ * the cells whose slots no halo message touches (full-array slabs: x in
+ * [1, nX-2]; list slabs: the inner tile range, except with FP16 storage,
+ * whose even step is not split and runs whole as part 1); part 1 the rest,
+ * after the phase-1 unpack and before the phase-0 pack. Returns 0 or an
+ * error code. */
+int lbm_aa_slab_even_part(KernelData *kd, CaseData *cd, int part, void *stream);
+
 /* The layout lbm_aa_list_slab_init builds, on the host only (no CUDA call):
  * counts[0..8] = owned nodes, ghost nodes, nCells, then the lengths of the
  * own / ghost slot lists of side 0 and of side 1 (-1: no halo), then the

@@ -290,6 +290,7 @@ lbm::AaArgs aa_args(Gpu* g) {
   a.haloHi = g->halo[1];
   a.crossLo = g->cross[0];
   a.crossHi = g->cross[1];
+  a.xBase = 0;
   const int S = (int)g->dstride;
   for (int d = 0; d < Q; ++d) {
     const int j = lbm::inv(d);
@@ -1213,6 +1214,49 @@ int lbm_aa_slab_step(KernelData* kd, CaseData* cd, int half, void* stream) {
     if (g->nGeneral > 0) lbm::aa_odd_interior_fp64(a, t, g->dOddBlocks + g->nDirect, 0, g->nGeneral, s);
     if (lbm::aa_shell_cells(a) > 0) lbm::aa_odd_face_fp64(a, t, s);
     g->iteration += 2;
+  }
+  return (int)cudaGetLastError();
+}
+
+int lbm_aa_slab_even_part(KernelData* kd, CaseData* cd, int part, void* stream) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  if (part < 0 || part > 1 || (g->kind != kAa && !g->listSlab)) return -1;
+  sync_upload(g);
+  const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
+  const cudaStream_t s = stream_or(g, stream);
+  if (g->listSlab) {
+    const int nTiles = (g->nFluid + lbm::kListTile - 1) / lbm::kListTile;
+    const bool split = g->innerT1 > g->innerT0 && g->storage != lbm::kStoreF16;
+    if (!split) {
+      // FP16 storage stages whole 1024-node tiles: the step is not split
+      if (part == 1) {
+        if (g->storage != lbm::kStoreF64)
+          lbm::list_even_lp(list_args_lp(g), to_float(t), g->storage, s);
+        else
+          lbm::list_even_fp64(list_args(g), t, s);
+      }
+      return (int)cudaGetLastError();
+    }
+    const int r[2][2] = {{part == 0 ? g->innerT0 : 0, part == 0 ? g->innerT1 : g->innerT0},
+                         {part == 0 ? 0 : g->innerT1, part == 0 ? 0 : nTiles}};
+    for (int k = 0; k < 2; ++k) {
+      if (r[k][1] <= r[k][0]) continue;
+      if (g->storage == lbm::kStoreF32)
+        lbm::list_even_lp_tiles(list_args_lp(g), to_float(t), r[k][0], r[k][1], s);
+      else
+        lbm::list_even_fp64_tiles(list_args(g), t, r[k][0], r[k][1], s);
+    }
+  } else {
+    const lbm::AaArgs a = aa_args(g);
+    const int nx = g->dims[0];
+    if (nx <= 2) {
+      if (part == 1) lbm::aa_even_fp64(a, t, s);
+    } else if (part == 0) {
+      lbm::aa_even_fp64_planes(a, t, 1, nx - 1, s);
+    } else {
+      lbm::aa_even_fp64_planes(a, t, 0, 1, s);
+      lbm::aa_even_fp64_planes(a, t, nx - 1, nx, s);
+    }
   }
   return (int)cudaGetLastError();
 }

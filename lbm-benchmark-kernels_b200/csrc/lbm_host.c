@@ -413,13 +413,18 @@ void lbmh_list_slab_inner_tiles(const LbmhListSlab *s, int tile, int *t0, int *t
 {
 	const int nOwned = s->nOwned;
 	const int nTiles = (nOwned + tile - 1) / tile;
-	/* a tile is inner when none of its nodes links to a ghost node */
+	/* a tile is inner when none of its nodes links to a ghost node and no
+	 * slot of its nodes is in an own list (a slot the neighbour reads and
+	 * writes) */
 	int lead = 0, trail = 0, inner = 1;
 	char *face = (char *)calloc(nTiles > 0 ? nTiles : 1, 1);
 	if (!face) { *t0 = *t1 = 0; return; }
 	for (long n = 0; n < nOwned; ++n)
 		for (int d = 0; d < 18; ++d)
 			if ((int)(s->adj[n * 18 + d] % (uint32_t)s->nCells) >= nOwned) { face[n / tile] = 1; break; }
+	for (int side = 0; side < 2; ++side)
+		for (long k = 0; s->own[side] && k < s->nOwnSlots[side]; ++k)
+			face[(s->own[side][k] % (uint32_t)s->nCells) / tile] = 1;
 	while (lead < nTiles && face[lead]) ++lead;
 	while (trail < nTiles - lead && face[nTiles - 1 - trail]) ++trail;
 	for (int t = lead; t < nTiles - trail; ++t) inner &= !face[t];

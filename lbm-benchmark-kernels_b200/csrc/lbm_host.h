@@ -62,8 +62,9 @@ int lbmh_list_slab_build(const LatticeDesc *ld, int x0, int x1, const int halo[2
 void lbmh_list_slab_free(LbmhListSlab *s);
 
 /* The slab's inner tiles (of `tile` owned nodes): [*t0, *t1), a contiguous
- * range of tiles none of whose nodes links to a ghost node, so that their
- * odd step reads and writes no halo slot. With the default numbering the
+ * range of tiles none of whose nodes links to a ghost node or owns a slot of
+ * an own list, so that neither their even nor their odd step touches a slot
+ * that a halo message carries. With the default numbering the
  * slab's two face planes are its first and last nodes and the range is the
  * rest; when face tiles are not all at the ends (blocked numbering), or
  * nothing is inner, the range is empty (0, 0). */

@@ -46,6 +46,7 @@ struct AaArgs {
   // mirrors (exchanged around the odd step); cross* marks a halo face that is
   // also the lattice's periodic x boundary. All 0 for a whole lattice.
   int haloLo, haloHi, crossLo, crossHi;
+  int xBase;  // even step: first x plane of the launch (grid z = planes launched)
 };
 
 // x-slab halo exchange (lbm_kernels_fp64.cu). A message is the 5 PDFs that
@@ -162,6 +163,12 @@ void list_odd_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStre
 // The odd steps over tiles [t0, t1) only (slabs overlap their halo exchange
 // with the tiles that read no ghost node).
 void list_odd_fp64_tiles(const ListArgs& a, const Trt<double>& t, int t0, int t1, cudaStream_t s);
+// The even steps over tiles [t0, t1) (FP64, and FP32 storage; the FP16 even
+// step stages whole 1024-node tiles and is not split) and the full-array
+// even step over x planes [x0, x1).
+void list_even_fp64_tiles(const ListArgs& a, const Trt<double>& t, int t0, int t1, cudaStream_t s);
+void list_even_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int t0, int t1, cudaStream_t s);
+void aa_even_fp64_planes(const AaArgs& a, const Trt<double>& t, int x0, int x1, cudaStream_t s);
 void list_odd_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int storage, int t0, int t1, cudaStream_t s);
 void aa_even_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
 // The AA odd step: the interior blocks (a list of nDirect blocks for the

@@ -71,7 +71,7 @@ __device__ __forceinline__ bool aa_open(const AaArgs& a, int x, int y, int z, in
 __global__ void __launch_bounds__(128, 8) k_aa_even_fp64(const AaArgs a, const Trt<double> t) {
   const int z = blockIdx.x * 128 + threadIdx.x;
   const int y = blockIdx.y;
-  const int x = blockIdx.z;
+  const int x = blockIdx.z + a.xBase;
   if (z >= a.nZ || y >= a.nY) return;
   const int c = aa_cell(a, x, y, z);
   if (!(__ldg(a.link + c) & kFluidBit)) return;
@@ -446,7 +446,16 @@ void aa_interior_blocks(const AaArgs& a, const uint32_t* link, int* blocks, int*
 }
 
 void aa_even_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
-  k_aa_even_fp64<<<dim3((a.nZ + 127) / 128, a.nY, a.nX), 128, 0, s>>>(a, t);
+  AaArgs b = a;
+  b.xBase = 0;
+  k_aa_even_fp64<<<dim3((a.nZ + 127) / 128, a.nY, a.nX), 128, 0, s>>>(b, t);
+}
+
+void aa_even_fp64_planes(const AaArgs& a, const Trt<double>& t, int x0, int x1, cudaStream_t s) {
+  if (x1 <= x0) return;
+  AaArgs b = a;
+  b.xBase = x0;
+  k_aa_even_fp64<<<dim3((a.nZ + 127) / 128, a.nY, x1 - x0), 128, 0, s>>>(b, t);
 }
 
 void aa_odd_interior_fp64(const AaArgs& a, const Trt<double>& t, const int* blocks, int nDirect, int nGeneral,
@@ -465,7 +474,7 @@ void aa_odd_face_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
 
 // 4 blocks of 256 threads per SM (64 registers, no spills)
 __global__ void __launch_bounds__(kListTile, 4) k_list_even_fp64(const ListArgs a, const Trt<double> t) {
-  const int n = blockIdx.x * kListTile + threadIdx.x;  // the even step is never split
+  const int n = (blockIdx.x + a.tileBase) * kListTile + threadIdx.x;
   if (n >= a.nFluid) return;
   double* const f = a.f + n;
   double* const fs = launder(f);
@@ -627,7 +636,16 @@ void slot_scatter(void* f, const uint32_t* idx, long long n, const void* buf, in
 static unsigned list_blocks(const ListArgs& a) { return (a.nFluid + kListTile - 1) / kListTile; }
 
 void list_even_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s) {
-  if (a.nFluid > 0) k_list_even_fp64<<<list_blocks(a), kListTile, 0, s>>>(a, t);
+  ListArgs b = a;
+  b.tileBase = 0;
+  if (a.nFluid > 0) k_list_even_fp64<<<list_blocks(b), kListTile, 0, s>>>(b, t);
+}
+
+void list_even_fp64_tiles(const ListArgs& a, const Trt<double>& t, int t0, int t1, cudaStream_t s) {
+  if (a.nFluid <= 0 || t1 <= t0) return;
+  ListArgs b = a;
+  b.tileBase = t0;
+  k_list_even_fp64<<<(unsigned)(t1 - t0), kListTile, 0, s>>>(b, t);
 }
 static std::atomic<int> g_oddAhead{0};
 

@@ -14,7 +14,7 @@ namespace lbm {
 template <class St>
 __global__ void __launch_bounds__(kListTile) k_list_even_lp(const ListArgsLp a, const Trt<float> t) {
   using T = typename St::T;
-  const int n = blockIdx.x * kListTile + threadIdx.x;
+  const int n = (blockIdx.x + a.tileBase) * kListTile + threadIdx.x;
   if (n >= a.nFluid) return;
   T* const f = static_cast<T*>(a.f) + n;
   T* const fs = launder(f);
@@ -175,10 +175,19 @@ static void launch_even_staged(const ListArgsLp& a, const Trt<float>& t, cudaStr
 // loads already keep enough bytes in flight (0.162 ms direct, 0.174 staged).
 void list_even_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s) {
   if (a.nFluid <= 0) return;
+  ListArgsLp b = a;
+  b.tileBase = 0;
   if (storage == kStoreF16)
-    launch_even_staged<StoreF16>(a, t, s);
+    launch_even_staged<StoreF16>(b, t, s);
   else
-    k_list_even_lp<StoreF32><<<lp_blocks(a), kListTile, 0, s>>>(a, t);
+    k_list_even_lp<StoreF32><<<lp_blocks(b), kListTile, 0, s>>>(b, t);
+}
+
+void list_even_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int t0, int t1, cudaStream_t s) {
+  if (a.nFluid <= 0 || t1 <= t0) return;
+  ListArgsLp b = a;
+  b.tileBase = t0;
+  k_list_even_lp<StoreF32><<<(unsigned)(t1 - t0), kListTile, 0, s>>>(b, t);
 }
 
 static std::atomic<int> ahead16{0}, ahead32{0};

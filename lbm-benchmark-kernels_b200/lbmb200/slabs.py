@@ -86,6 +86,7 @@ def _sigs(L):
         L.lbm_aa_slab_step.argtypes = [ctypes.POINTER(KernelData), ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         L.lbm_aa_slab_odd_part.argtypes = [ctypes.POINTER(KernelData), ctypes.c_void_p, ctypes.c_int,
                                            ctypes.c_void_p]
+        L.lbm_aa_slab_even_part.argtypes = L.lbm_aa_slab_odd_part.argtypes
         L._slab_sigs = True
     return L
 
@@ -144,6 +145,13 @@ class Slab:
         rc = self.L.lbm_aa_slab_odd_part(self.kdp, ctypes.byref(cd), int(part), stream)
         if rc:
             raise RuntimeError("slab odd step part failed (%d)" % rc)
+
+    def even_part(self, cd, part, stream=None):
+        """Part 0 (cells whose slots no message carries) or part 1 (the rest)
+        of the even step: lbm_aa_slab_even_part."""
+        rc = self.L.lbm_aa_slab_even_part(self.kdp, ctypes.byref(cd), int(part), stream)
+        if rc:
+            raise RuntimeError("slab even step part failed (%d)" % rc)
 
     def pack(self, side, phase, buf, stream=None):
         rc = self.L.lbm_aa_halo_pack(self.kdp, int(side), int(phase), _ptr(buf), stream)
@@ -295,23 +303,40 @@ def list_slab_layout(lattice, x0, x1, halo_lo, halo_hi, kernel_args=()):
 
 def step_pairs(slabs, transport, cd, pairs, stream=None, overlap=False):
     """`pairs` even/odd step pairs of a slab-decomposed lattice. With
-    `overlap`, the phase-0 messages travel while the cells that need no halo
-    data take their odd step (Slab.odd_part 0); the rest follows the unpack."""
-    for _ in range(pairs):
-        for s in slabs:
-            s.step(cd, 0, stream)
-        if overlap:
-            transport.start(0)
+    `overlap`, each exchange travels while the cells that its messages do not
+    concern take a step: the phase-0 messages during the odd step of the
+    inner cells (Slab.odd_part 0), the phase-1 messages during the next
+    pair's even step of the inner cells (Slab.even_part 0); the other cells
+    follow the unpack."""
+    if not overlap:
+        for _ in range(pairs):
             for s in slabs:
-                s.odd_part(cd, 0, stream)
-            transport.finish(0)
-            for s in slabs:
-                s.odd_part(cd, 1, stream)
-        else:
+                s.step(cd, 0, stream)
             transport.exchange(0)
             for s in slabs:
                 s.step(cd, 1, stream)
-        transport.exchange(1)
+            transport.exchange(1)
+        return
+    if pairs <= 0:
+        return
+    for s in slabs:
+        s.step(cd, 0, stream)
+    for k in range(pairs):
+        transport.start(0)
+        for s in slabs:
+            s.odd_part(cd, 0, stream)
+        transport.finish(0)
+        for s in slabs:
+            s.odd_part(cd, 1, stream)
+        transport.start(1)
+        last = k + 1 == pairs
+        if not last:
+            for s in slabs:
+                s.even_part(cd, 0, stream)
+        transport.finish(1)
+        if not last:
+            for s in slabs:
+                s.even_part(cd, 1, stream)
 
 
 def gather_field(slabs, lattice):

@@ -45,9 +45,7 @@ class EmuSlab:
     def half(self, oracle, odd):
         oracle.list_aa_half(odd, self.lay["n_owned"], self.nc, self.lay["adj"], self.f, OMEGA, LAM, XF)
 
-    def odd_part(self, oracle, part):
-        """Part 0 (the inner tiles, no ghost links) or part 1 (the rest) of
-        the odd step, by the library's inner tile range."""
+    def _part(self, oracle, odd, part):
         t0, t1 = self.lay["inner"]
         no = self.lay["n_owned"]
         if t1 > t0:
@@ -56,7 +54,16 @@ class EmuSlab:
             ranges = [] if part == 0 else [(0, no)]
         for n0, n1 in ranges:
             if n1 > n0:
-                oracle.list_aa_half_range(1, n0, n1, self.nc, self.lay["adj"], self.f, OMEGA, LAM, XF)
+                oracle.list_aa_half_range(odd, n0, n1, self.nc, self.lay["adj"], self.f, OMEGA, LAM, XF)
+
+    def odd_part(self, oracle, part):
+        """Part 0 (the inner tiles) or part 1 (the rest) of the odd step, by
+        the library's inner tile range."""
+        self._part(oracle, 1, part)
+
+    def even_part(self, oracle, part):
+        """The same split of the even step."""
+        self._part(oracle, 0, part)
 
     def idx(self, side, phase, pack):
         own = (phase == 0) == pack
@@ -86,9 +93,10 @@ def exchange(slabs, faces, phase):
 
 def run_slabs(oracle, lat, parts, pairs, init, kargs=(), overlap=False):
     """`pairs` step pairs of `lat` split into `parts` slabs in this process;
-    returns the gathered logical field and the slabs. With `overlap`, the
-    phase-0 messages are packed, then the inner tiles take their odd step,
-    then the messages are unpacked and the other tiles follow."""
+    returns the gathered logical field and the slabs. With `overlap`, each
+    phase's messages are packed, then the inner tiles take the next step
+    (odd after phase 0, the next even after phase 1), then the messages are
+    unpacked and the other tiles follow."""
     nx = lat.dims[0]
     ring = sl.is_ring(lat.periodic)
     slabs = []
@@ -102,24 +110,41 @@ def run_slabs(oracle, lat, parts, pairs, init, kargs=(), overlap=False):
         for phase in (0, 1):
             assert slabs[r].idx(1, phase, True).size == slabs[q].idx(0, phase, False).size
             assert slabs[q].idx(0, phase, True).size == slabs[r].idx(1, phase, False).size
-    for _ in range(pairs):
+    def send(phase):  # the packed messages, before any step that follows
+        return [(a.f[a.idx(1, phase, True)].copy(), b.f[b.idx(0, phase, True)].copy())
+                for a, b in ((slabs[r], slabs[q]) for r, q in faces)]
+
+    def receive(phase, sent):
+        for (r, q), (to_right, to_left) in zip(faces, sent):
+            slabs[q].f[slabs[q].idx(0, phase, False)] = to_right
+            slabs[r].f[slabs[r].idx(1, phase, False)] = to_left
+
+    if overlap:
         for s in slabs:
             s.half(oracle, 0)
-        if overlap:
-            sent = [(a.f[a.idx(1, 0, True)].copy(), b.f[b.idx(0, 0, True)].copy())
-                    for a, b in ((slabs[r], slabs[q]) for r, q in faces)]
+        for k in range(pairs):
+            sent = send(0)
             for s in slabs:
                 s.odd_part(oracle, 0)
-            for (r, q), (to_right, to_left) in zip(faces, sent):
-                slabs[q].f[slabs[q].idx(0, 0, False)] = to_right
-                slabs[r].f[slabs[r].idx(1, 0, False)] = to_left
+            receive(0, sent)
             for s in slabs:
                 s.odd_part(oracle, 1)
-        else:
+            sent = send(1)
+            if k + 1 < pairs:
+                for s in slabs:
+                    s.even_part(oracle, 0)
+            receive(1, sent)
+            if k + 1 < pairs:
+                for s in slabs:
+                    s.even_part(oracle, 1)
+    else:
+        for _ in range(pairs):
+            for s in slabs:
+                s.half(oracle, 0)
             exchange(slabs, faces, 0)
             for s in slabs:
                 s.half(oracle, 1)
-        exchange(slabs, faces, 1)
+            exchange(slabs, faces, 1)
     out = np.zeros_like(init)
     for s in slabs:
         s.get_field(out)

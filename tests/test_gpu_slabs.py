@@ -188,11 +188,14 @@ def test_slabrun_list_fp32_single_process(capsys):
     ("full", ["-lambda", "3/16"], "channel", (30, 12, 14), (0, 0, 0), 3),
     ("list", ["-lambda", "3/16", "-pad", "no"], "spheres", (30, 24, 24), (1, 1, 1), 3),
     ("list", ["-lambda", "3/16", "-precision", "fp32"], "spheres", (30, 24, 24), (1, 1, 1), 2),
+    ("list", ["-lambda", "3/16", "-precision", "fp16"], "spheres", (30, 24, 24), (1, 1, 1), 2),  # even step whole
     ("list", ["-lambda", "3/16", "-blk", "4"], "fluid", (16, 12, 12), (1, 1, 1), 2),  # no inner tile range
 ])
-def test_overlapped_odd_step_equals_whole_lattice(layout, kargs, geo, dims, per, parts):
-    """The odd step in two parts around the phase-0 exchange
-    (lbm_aa_slab_odd_part) leaves the single instance's bits."""
+def test_overlapped_steps_equal_whole_lattice(layout, kargs, geo, dims, per, parts):
+    """The odd step in two parts around the phase-0 exchange and the next
+    even step in two parts around the phase-1 exchange
+    (lbm_aa_slab_odd_part / lbm_aa_slab_even_part) leave the single
+    instance's bits."""
     lat = _lattice(geo, dims, per)
     rng = np.random.default_rng(8)
     init = lbmb200.W[None, :] * (1.0 + 0.05 * (rng.random((lat.mask.size, 19)) - 0.5))

@@ -97,17 +97,25 @@ LIST_SCRIPT = textwrap.dedent("""
     tr = sl.DistTransport(slab, r.rank, r.world, ring, dist, lambda n: torch.zeros(n, dtype=torch.float64))
     orc = Oracle()
     overlap = len(sys.argv) > 5 and sys.argv[5] == "1"
-    for _ in range(pairs):
+    if overlap:
         slab.half(orc, 0)
-        if overlap:
+        for k in range(pairs):
             tr.start(0)
             slab.odd_part(orc, 0)
             tr.finish(0)
             slab.odd_part(orc, 1)
-        else:
+            tr.start(1)
+            if k + 1 < pairs:
+                slab.even_part(orc, 0)
+            tr.finish(1)
+            if k + 1 < pairs:
+                slab.even_part(orc, 1)
+    else:
+        for _ in range(pairs):
+            slab.half(orc, 0)
             tr.exchange(0)
             slab.half(orc, 1)
-        tr.exchange(1)
+            tr.exchange(1)
     out = np.zeros((lat.mask.size, 19))
     slab.get_field(out)
     np.save(os.path.join(%(out)r, "part%%d.npy" %% r.rank), out[slab.gcells])
