@@ -12,7 +12,8 @@ list (cuda-list-aa-pv-soa kernels) -- and runs `pairs` even/odd step pairs;
 rank 0 prints the aggregate MFLUP/s (device-timed per rank with CUDA events,
 max over ranks). List slabs (any --precision) also report the FP64
 conservation sums of the whole lattice (per-slab sums all-reduced) and the
-permeability they give.
+permeability they give. --overlap sends each phase's halo messages while
+the cells they do not concern take their step (Slab.odd_part/even_part).
 With one process, the lattice runs as one slab without halos.
 """
 import argparse

@@ -175,10 +175,10 @@ def test_reduced_storage_list_slabs_equal_whole_lattice(prec, geo, dims, per, pa
 def test_slabrun_list_fp32_single_process(capsys):
     from lbmb200 import slabrun
     slabrun.main(["--dims", "32x24x24", "--geometry", "spheres:7:0.5:2:4", "--layout", "list",
-                  "--precision", "fp32", "--pairs", "2", "--warmup", "1"])
+                  "--precision", "fp32", "--pairs", "2", "--warmup", "1", "--overlap"])
     import json
     rec = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
-    assert rec["precision"] == "fp32" and rec["mflups"] > 0
+    assert rec["precision"] == "fp32" and rec["overlap"] and rec["mflups"] > 0
     assert abs(rec["sum_rho"] - rec["fluid_nodes"]) < 1e-6 * rec["fluid_nodes"]
     assert rec["sum_jx"] > 0 and rec["permeability"] > 0
 
