@@ -325,8 +325,8 @@ int lbm_aa_slab_odd_part(KernelData *kd, CaseData *cd, int part, void *stream);
 /* The even step (half 0) in the same two parts, so that the phase-1
  * messages of the previous pair can travel while part 0 runs: part 0 updates
  * the cells whose slots no halo message touches (full-array slabs: x in
- * [1, nX-2]; list slabs: the inner tile range, except with FP16 storage,
- * whose even step is not split and runs whole as part 1); part 1 the rest,
+ * [1, nX-2]; list slabs: the inner tile range; with FP16 storage both parts
+ * use the per-node even kernel instead of the staged one); part 1 the rest,
  * after the phase-1 unpack and before the phase-0 pack. Returns 0 or an
  * error code. */
 int lbm_aa_slab_even_part(KernelData *kd, CaseData *cd, int part, void *stream);

@@ -1226,9 +1226,8 @@ int lbm_aa_slab_even_part(KernelData* kd, CaseData* cd, int part, void* stream) 
   const cudaStream_t s = stream_or(g, stream);
   if (g->listSlab) {
     const int nTiles = (g->nFluid + lbm::kListTile - 1) / lbm::kListTile;
-    const bool split = g->innerT1 > g->innerT0 && g->storage != lbm::kStoreF16;
+    const bool split = g->innerT1 > g->innerT0;
     if (!split) {
-      // FP16 storage stages whole 1024-node tiles: the step is not split
       if (part == 1) {
         if (g->storage != lbm::kStoreF64)
           lbm::list_even_lp(list_args_lp(g), to_float(t), g->storage, s);
@@ -1241,8 +1240,8 @@ int lbm_aa_slab_even_part(KernelData* kd, CaseData* cd, int part, void* stream) 
                          {part == 0 ? 0 : g->innerT1, part == 0 ? 0 : nTiles}};
     for (int k = 0; k < 2; ++k) {
       if (r[k][1] <= r[k][0]) continue;
-      if (g->storage == lbm::kStoreF32)
-        lbm::list_even_lp_tiles(list_args_lp(g), to_float(t), r[k][0], r[k][1], s);
+      if (g->storage != lbm::kStoreF64)
+        lbm::list_even_lp_tiles(list_args_lp(g), to_float(t), g->storage, r[k][0], r[k][1], s);
       else
         lbm::list_even_fp64_tiles(list_args(g), t, r[k][0], r[k][1], s);
     }

@@ -163,11 +163,11 @@ void list_odd_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStre
 // The odd steps over tiles [t0, t1) only (slabs overlap their halo exchange
 // with the tiles that read no ghost node).
 void list_odd_fp64_tiles(const ListArgs& a, const Trt<double>& t, int t0, int t1, cudaStream_t s);
-// The even steps over tiles [t0, t1) (FP64, and FP32 storage; the FP16 even
-// step stages whole 1024-node tiles and is not split) and the full-array
-// even step over x planes [x0, x1).
+// The even steps over tiles [t0, t1) (reduced storage: the per-node kernel,
+// also for FP16, whose whole-array step is the staged kernel) and the
+// full-array even step over x planes [x0, x1).
 void list_even_fp64_tiles(const ListArgs& a, const Trt<double>& t, int t0, int t1, cudaStream_t s);
-void list_even_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int t0, int t1, cudaStream_t s);
+void list_even_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int storage, int t0, int t1, cudaStream_t s);
 void aa_even_fp64_planes(const AaArgs& a, const Trt<double>& t, int x0, int x1, cudaStream_t s);
 void list_odd_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int storage, int t0, int t1, cudaStream_t s);
 void aa_even_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);

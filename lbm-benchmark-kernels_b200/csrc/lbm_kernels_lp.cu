@@ -183,11 +183,16 @@ void list_even_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStr
     k_list_even_lp<StoreF32><<<lp_blocks(b), kListTile, 0, s>>>(b, t);
 }
 
-void list_even_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int t0, int t1, cudaStream_t s) {
+// Tile ranges run the per-node kernel for both storages (the FP16 staged
+// kernel works on whole 1024-node tiles).
+void list_even_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int storage, int t0, int t1, cudaStream_t s) {
   if (a.nFluid <= 0 || t1 <= t0) return;
   ListArgsLp b = a;
   b.tileBase = t0;
-  k_list_even_lp<StoreF32><<<(unsigned)(t1 - t0), kListTile, 0, s>>>(b, t);
+  if (storage == kStoreF16)
+    k_list_even_lp<StoreF16><<<(unsigned)(t1 - t0), kListTile, 0, s>>>(b, t);
+  else
+    k_list_even_lp<StoreF32><<<(unsigned)(t1 - t0), kListTile, 0, s>>>(b, t);
 }
 
 static std::atomic<int> ahead16{0}, ahead32{0};
