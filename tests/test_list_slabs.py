@@ -164,3 +164,8 @@ def test_inner_tiles_link_to_no_ghost():
         adj = lay["adj"].reshape(-1, 18)
         inner = adj[t0 * 256: min(t1 * 256, lay["n_owned"])]
         assert np.all(inner % lay["n_cells"] < lay["n_owned"])
+        # no slot of an inner node travels in a message
+        for own in lay["own"]:
+            if own is not None:
+                node = own % lay["n_cells"]
+                assert not np.any((node >= t0 * 256) & (node < t1 * 256))
