@@ -229,12 +229,42 @@ long lbm_b200_last_launches(KernelData *kd);
  * upload of a dirty mirror, download after the steps). */
 void lbm_b200_last_copy_bytes(KernelData *kd, size_t *h2d, size_t *d2h);
 
+/* Lost device state. The kernels' bounded waits (bulk copies into shared
+ * memory) give up after a fixed number of polls and set a device error word
+ * instead of hanging; a skipped tile sets it too. The calls below that read
+ * the word (sync_mirror, time_steps, instance_moments, checkpoint_save, and
+ * Kernel, which exits) then mark the instance's device state as lost: a copy
+ * that arrived late may have landed in another block's shared memory, so
+ * none of that launch's results can be trusted. While the state is lost,
+ * every step entry point refuses with -4 (Kernel exits with a message),
+ * sync_mirror keeps the mirror at the last good state and returns -4, and
+ * checkpoint_save writes nothing (-4). Uploading a host state (set_field,
+ * SetNode edits followed by a step call, or checkpoint_load) clears it. */
+
+/* The -verify check of KernelVerifiy (src/Kernel.c:456-625) on the device:
+ * the x-velocity slice at x = nX/2 and the Poiseuille L2 relative error,
+ * summed over z with warp shuffles, from the instance's device PDFs (after
+ * its pending steps; a dirty mirror is uploaded first). Moves only the nY x
+ * nZ slice and the error to the host -- not the field, as a GetNode-based
+ * check after a device-only run would. *err = the error norm; with
+ * write_file also the reference's flow-profile.dat. Returns 0, -1 for a
+ * lattice of other dimensions, -4 on a lost device state, or a CUDA error
+ * code. */
+int lbm_b200_verify_device(LatticeDesc *ld, KernelData *kd, CaseData *cd, int write_file, double *err);
+
+/* Test hook for the rule above: writes `word` into the instance's device
+ * error word from the host (after its pending work), as a bounded wait that
+ * gave up would have; no kernel runs and nothing faults. Returns 0 or a CUDA
+ * error code. */
+int lbm_b200_inject_device_error(KernelData *kd, int word);
+
 /* Runs n time steps without touching the host mirror (no upload, no download,
  * no synchronisation), for callers that keep the state on the device. Returns
- * 0, or a CUDA error code. */
+ * 0, -4 on a lost device state, or a CUDA error code. */
 int lbm_b200_step_device(KernelData *kd, CaseData *cd, int n);
 
-/* Copies the device state into the host mirror (blocking). */
+/* Copies the device state into the host mirror (blocking); -4 (mirror
+ * unchanged) on a lost device state. */
 int lbm_b200_sync_mirror(KernelData *kd);
 
 /* Marks the host mirror as changed, so the next Kernel call uploads it. */
@@ -242,8 +272,9 @@ void lbm_b200_mark_mirror_dirty(KernelData *kd);
 
 /* Runs n time steps on the device and times them with CUDA events on the
  * instance's stream: *total_ms for the whole sequence, per_launch_ms[k]
- * (optional, n entries) for launch k. No mirror traffic. Returns 0 or a CUDA
- * error code. */
+ * (optional, n entries) for launch k. No mirror traffic. Returns 0, -1 when
+ * the device error word is set after the steps, -4 on a lost device state,
+ * or a CUDA error code. */
 int lbm_b200_time_steps(KernelData *kd, CaseData *cd, int n, double *total_ms, double *per_launch_ms);
 
 /* Number of kernel launches that n time steps take on this instance (the
@@ -375,17 +406,20 @@ int lbm_b200_moments_device(const double *pdfs, long long nCells, int nFluid, do
 /* The same sums for a list-kernel instance, into host memory (out[0..3]);
  * waits for the instance's pending steps. With FP32/FP16 storage the stored
  * deviations from the weights are summed in FP64 and the node count added to
- * the mass. Returns 0, -1 for the full-array kernels, or a CUDA error code. */
+ * the mass. Returns 0, -1 for the full-array kernels, -4 on a lost device
+ * state, or a CUDA error code. */
 int lbm_b200_instance_moments(KernelData *kd, double *out);
 
 /* Checkpoint / restart of an instance (no counterpart in the reference):
  * _save writes the current state -- a header (kernel, storage, lattice
- * dimensions and periodicity, step parity, Lambda; host byte order) and the
- * PDF array exactly as the device holds it, with an FNV-1a checksum; pending
- * SetNode edits are part of the state. _load restores it into an instance of
- * the same kernel, storage, lattice and Lambda, so that the run continues
- * bit for bit. Return 0; -1 I/O error; -2 the file does not match the
- * instance; -3 checksum mismatch (state unchanged); or a CUDA error code. */
+ * dimensions and periodicity, a hash of the lattice mask, step parity,
+ * Lambda; host byte order) and the PDF array exactly as the device holds it,
+ * with an FNV-1a checksum; pending SetNode edits are part of the state. _load
+ * restores it into an instance of the same kernel, storage, lattice
+ * (geometry, not only its counts) and Lambda, so that the run continues bit
+ * for bit. Return 0; -1 I/O error; -2 the file does not match the instance;
+ * -3 checksum mismatch (state unchanged); -4 (_save) on a lost device state;
+ * or a CUDA error code. */
 int lbm_b200_checkpoint_save(KernelData *kd, const char *path);
 int lbm_b200_checkpoint_load(KernelData *kd, const char *path);
 
@@ -411,9 +445,12 @@ int lbm_b200_list_layout(KernelData *kd, const uint32_t **grid, const uint32_t *
  * accepts at most 16,777,216 fluid nodes and returns -2 (with a message) above
  * that. Allocates nothing; does not synchronise (the result is ready when the
  * stream is). The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) and should come before any stream capture. Calls
- * share the array: calls that overlap on the GPU race. Returns 0, -1 for bad
- * arguments, or a CUDA error code. */
+ * (cudaGetSymbolAddress) and should come before any stream capture; the
+ * address is cached for the process, which assumes the device's context is
+ * not reset (cudaDeviceReset) meanwhile. Calls share the array: calls that
+ * overlap on the GPU race. A CUDA error already pending from earlier work is
+ * returned without enqueueing anything. Returns 0, -1 for bad arguments, or a
+ * CUDA error code. */
 int lbm_b200_moments_noalloc(const double *pdfs, long long nCells, int nFluid, double *out_device, void *stream);
 
 /* Host layout builders (no GPU needed), exported for the parity tests:

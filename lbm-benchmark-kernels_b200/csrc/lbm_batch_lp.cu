@@ -28,12 +28,7 @@ __device__ __forceinline__ void tile_store(BatchTile* dst, uint32_t w) {
 
 template <class St>
 __device__ __forceinline__ void batch_even_node(const BatchTile& T, int n) {
-  using T_ = typename St::T;
-  T_* const f = static_cast<T_*>(T.f) + n;
-  T_* const fs = launder(f);
-  const long long S = T.nCells;
-  trt_update(T.trt, [&](int d) { return St::dev(f[d * S], d); },
-             [&](int d, float v) { fs[inv(d) * S] = St::raw(v, inv(d)); });
+  lp_even_node<St>(static_cast<typename St::T*>(T.f), T.nCells, n, TrtDev<St>(T.trt));
 }
 
 // Grid-stride over the tiles; with one block per tile the loop runs once.
@@ -70,27 +65,10 @@ __global__ void __launch_bounds__(256) k_batch_even(const BatchArgs a) {
 // index in the tile): link d is e[d] + off.
 template <class St>
 __device__ __forceinline__ void batch_odd_node(const BatchTile& T, const uint32_t* srun, int local) {
-  using T_ = typename St::T;
   uint32_t off;
   const uint32_t* e = run_row(srun, local, off);
-  const int n = T.n0 + local;
-  T_* const f = static_cast<T_*>(T.f);
-  const long long S = T.nCells;
-  const TrtW& t = T.trt;
-  auto load = [&](int d) -> float {
-    return St::dev(d == DC ? f[DC * S + n] : f[e[inv(d)] + off], d) + t.force(d);
-  };
-  auto store = [&](int d, float v) {
-    if (d == DC) {
-      f[DC * S + n] = St::raw(v + t.force(DC), DC);
-      return;
-    }
-    const uint32_t dst = reinterpret_cast<const volatile uint32_t*>(e)[d] + off;
-    const int j = inv(d);
-    const bool bounce = dst == static_cast<uint32_t>(j * S + n);
-    f[dst] = St::raw(v + (bounce ? t.force(j) : t.force(d)), d);
-  };
-  trt_update(t, load, store);
+  lp_odd_node<St>(static_cast<typename St::T*>(T.f), static_cast<uint32_t>(T.nCells), T.n0 + local, e, off,
+                  TrtDev<St>(T.trt));
 }
 
 static_assert(kBatchTileNodes == kListTile, "batch tiles are the run records' tiles");
@@ -179,8 +157,10 @@ __global__ void __launch_bounds__(kBatchTileNodes / NPT) k_batch_even_tile(const
   }
 }
 
+// 6 tiles' blocks resident per SM (the shared-memory limit of the staged run
+// records), which caps the registers at 40.
 template <class St, int NPT>
-__global__ void __launch_bounds__(kBatchTileNodes / NPT) k_batch_odd_tile(const BatchArgs a) {
+__global__ void __launch_bounds__(kBatchTileNodes / NPT, 6 * NPT) k_batch_odd_tile(const BatchArgs a) {
   __shared__ __align__(128) uint32_t srun[kRunTileWords];
   __shared__ alignas(8) uint64_t bar;
   __shared__ __align__(16) BatchTile st;

@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <vector>
 #include <strings.h>
 
 #include "../../include/lbm_b200.h"
@@ -63,14 +64,24 @@ struct Gpu {
   uint32_t* dLink;
   uint32_t* dAdj;
   int* dErr;
+  // Set once the device error word was found non-zero: a bounded wait gave up
+  // (bit 1; a bulk copy may still have landed in another block's shared
+  // memory) or a tile was skipped (bit 4), so the device PDFs are not a state
+  // of the update. Steps are refused until the host state is uploaded again
+  // (set_field / SetNode, or a checkpoint restore), which clears it.
+  bool stateLost;
+  uint64_t maskHash;       // FNV-1a of the instance's lattice mask (checkpoint check)
+  double* dVerify;         // device -verify: x-velocity slice (nY*nZ) + the error
+  long long* dVerifyBase;  // device -verify: element base of each slice cell
   cudaStream_t stream;
   cudaEvent_t ev0, ev1;
 
   // AA layout
   int xs, pitch;
   long long dstride;
-  int* dOddBlocks;         // interior blocks of the odd step: nDirect direct, then nGeneral general
-  int nDirect, nGeneral;
+  int* dOddItems;          // odd step: nOddItems interior work items (aa_interior_items)
+  int* dOddCells;          // odd step: the general cells of the items, in chunks of 128
+  int nOddItems;
   // x-slab of a larger lattice (lbm_aa_slab_init): halo/cross flags of the two x faces
   int halo[2], cross[2];
   int* sliceMask;          // the slab's own mask (owned)
@@ -193,18 +204,15 @@ lbm::Trt<double> make_trt(double omega, double lambda, double xforce) {
   return t;
 }
 
-lbm::Trt<float> to_float(const lbm::Trt<double>& d) {
-  lbm::Trt<float> t;
+// The reduced-storage kernels' constants: the two rates and the x body force
+// as its two class increments (the FP32 values of the FP64 table's E and NE
+// entries).
+lbm::TrtW to_trtw(const lbm::Trt<double>& d) {
+  lbm::TrtW t;
   t.omegaEven = (float)d.omegaEven;
   t.omegaOdd = (float)d.omegaOdd;
-  t.w0 = (float)d.w0;
-  t.w1 = (float)d.w1;
-  t.w2 = (float)d.w2;
-  t.w1x3 = (float)d.w1x3;
-  t.w2x3 = (float)d.w2x3;
-  t.w1nh = (float)d.w1nh;
-  t.w2nh = (float)d.w2nh;
-  for (int k = 0; k < Q; ++k) t.force[k] = (float)d.force[k];
+  t.fx1 = (float)d.force[lbm::E];
+  t.fx2 = (float)d.force[lbm::NE];
   return t;
 }
 
@@ -360,14 +368,9 @@ long enqueue_steps(Gpu* g, const lbm::Trt<double>& t, int n, cudaEvent_t* ev = n
       mark();
       lbm::aa_even_fp64(a, t, g->stream);
       ++k;
-      if (g->nDirect > 0) {
+      if (g->nOddItems > 0) {
         mark();
-        lbm::aa_odd_interior_fp64(a, t, g->dOddBlocks, g->nDirect, 0, g->stream);
-        ++k;
-      }
-      if (g->nGeneral > 0) {
-        mark();
-        lbm::aa_odd_interior_fp64(a, t, g->dOddBlocks + g->nDirect, 0, g->nGeneral, g->stream);
+        lbm::aa_odd_interior_fp64(a, t, g->dOddItems, g->nOddItems, g->dOddCells, g->stream);
         ++k;
       }
       if (shell) {
@@ -379,7 +382,7 @@ long enqueue_steps(Gpu* g, const lbm::Trt<double>& t, int n, cudaEvent_t* ev = n
     }
   } else if (g->kind == kListAa && g->storage != lbm::kStoreF64) {
     const lbm::ListArgsLp a = list_args_lp(g);
-    const lbm::Trt<float> tf = to_float(t);
+    const lbm::TrtW tf = to_trtw(t);
     for (int it = 0; it < n; it += 2) {
       mark();
       lbm::list_even_lp(a, tf, g->storage, g->stream);
@@ -434,7 +437,7 @@ long launches_for(Gpu* g, int n) {
   long perPair = 2;
   if (g->kind == kAa) {
     const lbm::AaArgs a = aa_args(g);
-    perPair = 1 + (g->nDirect > 0) + (g->nGeneral > 0) + (lbm::aa_shell_cells(a) > 0 ? 1 : 0);
+    perPair = 1 + (g->nOddItems > 0) + (lbm::aa_shell_cells(a) > 0 ? 1 : 0);
   }
   return perPair * ((n + 1) / 2);
 }
@@ -469,6 +472,14 @@ void raw_to_mirror(Gpu* g) {
   }
 }
 
+// A fresh host state is on its way to the device: the error word and the
+// lost flag start over (stream-ordered after the upload).
+void clear_lost(Gpu* g) {
+  if (!g->stateLost) return;
+  LBM_CK(cudaMemsetAsync(g->dErr, 0, sizeof(int), g->stream));
+  g->stateLost = false;
+}
+
 void upload_if_dirty(Gpu* g) {
   g->lastH2D = 0;
   if (!g->dirty) return;
@@ -481,6 +492,7 @@ void upload_if_dirty(Gpu* g) {
   LBM_CK(cudaMemcpyAsync(current_grid(g), src, g->mirrorElems * g->elemBytes, cudaMemcpyHostToDevice, g->stream));
   g->lastH2D = g->mirrorElems * g->elemBytes;
   g->dirty = false;
+  clear_lost(g);
 }
 
 void download(Gpu* g) {
@@ -491,14 +503,32 @@ void download(Gpu* g) {
   g->lastD2H = g->mirrorElems * g->elemBytes;
 }
 
-void check_device_error(Gpu* g) {
+// Reads the device error word (synchronous); a non-zero word marks the
+// device state as lost. Returns the word.
+int read_device_error(Gpu* g) {
   int err = 0;
   LBM_CK(cudaMemcpy(&err, g->dErr, sizeof(int), cudaMemcpyDeviceToHost));
   if (err) {
-    g_lastError = "a device wait exceeded its limit (error word " + std::to_string(err) + ")";
+    g->stateLost = true;
+    g_lastError = "a device wait exceeded its limit or a tile was skipped (error word " + std::to_string(err) +
+                  "); the device state is lost until the host state is uploaded again";
+  }
+  return err;
+}
+
+void check_device_error(Gpu* g) {
+  if (read_device_error(g)) {
     std::printf("ERROR: %s\n", g_lastError.c_str());
     std::exit(1);
   }
+}
+
+// Steps refuse to run on a lost device state (see Gpu::stateLost).
+bool refuse_lost(Gpu* g) {
+  if (!g->stateLost) return false;
+  g_lastError = "the device state was lost to an earlier device error; upload a state (set_field, SetNode or a "
+                "checkpoint restore) before stepping";
+  return true;
 }
 
 void vtk_or_exit(LatticeDesc* ld, KernelData* kd, CaseData* cd, int label) {
@@ -536,6 +566,10 @@ void cb_kernel(LatticeDesc* ld, KernelData* kd, CaseData* cd) {
   // the two-grid full-array kernels label their first file 0 (src/BenchKernelD3Q19.c:98-101)
   if (cd->VtkOutput) vtk_or_exit(ld, kd, cd, (g->kind == kFaPush || g->kind == kFaPull) ? 0 : -1);
   upload_if_dirty(g);
+  if (refuse_lost(g)) {
+    std::printf("ERROR: %s\n", g_lastError.c_str());
+    std::exit(1);
+  }
   const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
 
   LBM_CK(cudaStreamSynchronize(g->stream));
@@ -565,6 +599,8 @@ struct SlabSpec {
   LbmhListSlab* list;  // list layout of a list-AA slab (ownership moves to the instance)
 };
 
+uint64_t fnv1a64(const void* data, size_t n);
+
 Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* slab = nullptr) {
   Gpu* g = static_cast<Gpu*>(std::calloc(1, sizeof(Gpu)));
   if (!g) { std::printf("ERROR: allocation failed.\n"); std::exit(1); }
@@ -578,6 +614,7 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* sla
     std::exit(1);
   }
   g->iteration = -1;
+  g->maskHash = fnv1a64(ld->Lattice, sizeof(int) * (size_t)ld->Dims[0] * ld->Dims[1] * ld->Dims[2]);
   for (int i = 0; i < 3; ++i) g->dims[i] = ld->Dims[i];
   g->per[0] = ld->PeriodicX;
   g->per[1] = ld->PeriodicY;
@@ -646,19 +683,20 @@ Gpu* gpu_new(Kind kind, LatticeDesc* ld, Parameters* params, const SlabSpec* sla
       LBM_CK(cudaMalloc(&g->dG, sizeof(double) * g->mirrorElems));
       LBM_CK(cudaMemset(g->dG, 0, sizeof(double) * g->mirrorElems));
     }
-    // the AA odd step's interior blocks, direct ones first
+    // the AA odd step's interior work items
     const lbm::AaArgs aa = aa_args(g);
-    const long long nb = kind == kAa ? lbm::aa_interior_block_count(aa) : 0;
-    if (nb > 0) {
-      int* blocks = static_cast<int*>(std::malloc(sizeof(int) * (size_t)nb));
-      if (!blocks) { std::printf("ERROR: allocation failed.\n"); std::exit(1); }
-      lbm::aa_interior_blocks(aa, link, blocks, &g->nDirect, &g->nGeneral);
-      if (g->nDirect + g->nGeneral > 0) {
-        LBM_CK(cudaMalloc(&g->dOddBlocks, sizeof(int) * (size_t)(g->nDirect + g->nGeneral)));
-        LBM_CK(cudaMemcpy(g->dOddBlocks, blocks, sizeof(int) * (size_t)(g->nDirect + g->nGeneral),
-                          cudaMemcpyHostToDevice));
+    if (kind == kAa && lbm::aa_interior_block_count(aa) > 0) {
+      std::vector<int> items, cells;
+      lbm::aa_interior_items(aa, link, items, cells);
+      g->nOddItems = (int)items.size();
+      if (!items.empty()) {
+        LBM_CK(cudaMalloc(&g->dOddItems, sizeof(int) * items.size()));
+        LBM_CK(cudaMemcpy(g->dOddItems, items.data(), sizeof(int) * items.size(), cudaMemcpyHostToDevice));
       }
-      std::free(blocks);
+      if (!cells.empty()) {
+        LBM_CK(cudaMalloc(&g->dOddCells, sizeof(int) * cells.size()));
+        LBM_CK(cudaMemcpy(g->dOddCells, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice));
+      }
     }
     std::free(link);
   } else {
@@ -769,7 +807,10 @@ void gpu_free(KernelData** kernelData) {
   cudaFree(g->dF);
   cudaFree(g->dG);
   cudaFree(g->dLink);
-  cudaFree(g->dOddBlocks);
+  cudaFree(g->dOddItems);
+  cudaFree(g->dVerify);
+  cudaFree(g->dVerifyBase);
+  cudaFree(g->dOddCells);
   std::free(g->sliceMask);
   cudaFree(g->dAdj);
   cudaFree(g->dRuns);
@@ -806,17 +847,18 @@ uint64_t fnv1a64(const void* data, size_t n) {
 // Instance checkpoint: this header (host byte order), then the current PDF
 // array exactly as the device holds it (storage format, padding included).
 struct CkptHeader {
-  char magic[8];  // "LBMCKPT1"
+  char magic[8];  // "LBMCKPT2"
   int32_t kind, storage;
   int32_t dims[3], per[3];
   int32_t iteration, nFluid;
   int64_t elems;
   int32_t elemBytes, reserved;
   double lambda;
+  uint64_t maskHash;  // FNV-1a of the lattice mask: the same geometry, not only the same counts
   uint64_t checksum;
 };
 
-const char kCkptMagic[8] = {'L', 'B', 'M', 'C', 'K', 'P', 'T', '1'};
+const char kCkptMagic[8] = {'L', 'B', 'M', 'C', 'K', 'P', 'T', '2'};
 
 CkptHeader ckpt_header_of(const Gpu* g) {
   CkptHeader h;
@@ -833,6 +875,7 @@ CkptHeader ckpt_header_of(const Gpu* g) {
   h.elems = (int64_t)g->mirrorElems;
   h.elemBytes = (int32_t)g->elemBytes;
   h.lambda = g->lambda;
+  h.maskHash = g->maskHash;
   return h;
 }
 
@@ -944,9 +987,75 @@ void lbm_b200_last_copy_bytes(KernelData* kd, size_t* h2d, size_t* d2h) {
 int lbm_b200_step_device(KernelData* kd, CaseData* cd, int n) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
   if (g->dirty) upload_if_dirty(g);
+  if (refuse_lost(g)) return -4;
   const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
   g->lastLaunches = enqueue_steps(g, t, n);
   cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) g_lastError = cudaGetErrorString(e);
+  return (int)e;
+}
+
+int lbm_b200_verify_device(LatticeDesc* ld, KernelData* kd, CaseData* cd, int write_file, double* err) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  const int nx = g->dims[0], ny = g->dims[1], nz = g->dims[2];
+  if (ld->Dims[0] != nx || ld->Dims[1] != ny || ld->Dims[2] != nz || !err) return -1;
+  if (g->dirty) upload_if_dirty(g);
+  if (refuse_lost(g)) return -4;
+  const size_t n = (size_t)ny * nz;
+  // element base of each slice cell (x = nX/2) in the instance's layout
+  std::vector<long long> base(n);
+  const int xs = nx / 2;
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y) {
+      long long b = -1;
+      if (ld->Lattice[lbmh_lidx(ld->Dims, xs, y, z)] != LAT_CELL_OBSTACLE)
+        b = full_array(g->kind) ? (long long)(xs + 1) * g->xs + (long long)(y + 1) * g->pitch + z + lbm::kZOff
+                                : (long long)g->grid[lbmh_lidx(ld->Dims, xs, y, z)];
+      base[(size_t)y * nz + z] = b;
+    }
+  lbm::VerifyArgs a;
+  a.f = current_grid(g);
+  a.storage = g->storage;
+  a.nY = ny;
+  a.nZ = nz;
+  a.xforce = cd->XForce;
+  a.visc = (1.0 / cd->Omega - 0.5) / 3.0;
+  for (int d = 0; d < Q; ++d) {
+    if (full_array(g->kind)) {
+      a.off[d] = (long long)d * g->dstride;
+      // pull-soa keeps node x's PDF d at x - c_d (as GetNode)
+      if (g->kind == kFaPull) a.off[d] -= (long long)lbm::cx(d) * g->xs + (long long)lbm::cy(d) * g->pitch + lbm::cz(d);
+    } else {
+      a.off[d] = (long long)d * g->nCells;
+    }
+  }
+  cudaError_t e = cudaSuccess;
+  if (!g->dVerify) e = cudaMalloc(&g->dVerify, sizeof(double) * (n + 1));
+  if (e == cudaSuccess && !g->dVerifyBase) e = cudaMalloc(&g->dVerifyBase, sizeof(long long) * n);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(g->dVerifyBase, base.data(), sizeof(long long) * n, cudaMemcpyHostToDevice, g->stream);
+  if (e == cudaSuccess) {
+    a.base = g->dVerifyBase;
+    lbm::verify_device(a, g->dVerify, g->dVerify + n, g->stream);
+    e = cudaGetLastError();
+  }
+  // only the slice and the error come back
+  std::vector<double> slice(n + 1);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(slice.data(), g->dVerify, sizeof(double) * (n + 1), cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  if (e != cudaSuccess) { g_lastError = cudaGetErrorString(e); return (int)e; }
+  if (read_device_error(g)) return -4;
+  g->lastD2H = sizeof(double) * (n + 1);
+  *err = slice[n];
+  if (write_file) lbmh_verify_profile(ny, nz, cd->Omega, cd->XForce, slice.data(), 1);
+  return 0;
+}
+
+int lbm_b200_inject_device_error(KernelData* kd, int word) {
+  Gpu* g = reinterpret_cast<Gpu*>(kd);
+  cudaError_t e = cudaStreamSynchronize(g->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(g->dErr, &word, sizeof(int), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) g_lastError = cudaGetErrorString(e);
   return (int)e;
 }
@@ -955,6 +1064,8 @@ int lbm_b200_sync_mirror(KernelData* kd) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
   cudaError_t e = cudaStreamSynchronize(g->stream);
   if (e != cudaSuccess) { g_lastError = cudaGetErrorString(e); return (int)e; }
+  // a lost device state is not downloaded: the mirror keeps the last good one
+  if (g->stateLost || read_device_error(g)) return -4;
   download(g);
   return 0;
 }
@@ -1183,11 +1294,12 @@ int lbm_aa_slab_step(KernelData* kd, CaseData* cd, int half, void* stream) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
   if (half < 0 || half > 1 || (g->kind != kAa && !g->listSlab)) return -1;
   sync_upload(g);
+  if (refuse_lost(g)) return -4;
   const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
   const cudaStream_t s = stream_or(g, stream);
   if (g->listSlab && g->storage != lbm::kStoreF64) {
     const lbm::ListArgsLp la = list_args_lp(g);
-    const lbm::Trt<float> tf = to_float(t);
+    const lbm::TrtW tf = to_trtw(t);
     if (half == 0) {
       lbm::list_even_lp(la, tf, g->storage, s);
     } else {
@@ -1210,8 +1322,7 @@ int lbm_aa_slab_step(KernelData* kd, CaseData* cd, int half, void* stream) {
   if (half == 0) {
     lbm::aa_even_fp64(a, t, s);
   } else {
-    if (g->nDirect > 0) lbm::aa_odd_interior_fp64(a, t, g->dOddBlocks, g->nDirect, 0, s);
-    if (g->nGeneral > 0) lbm::aa_odd_interior_fp64(a, t, g->dOddBlocks + g->nDirect, 0, g->nGeneral, s);
+    if (g->nOddItems > 0) lbm::aa_odd_interior_fp64(a, t, g->dOddItems, g->nOddItems, g->dOddCells, s);
     if (lbm::aa_shell_cells(a) > 0) lbm::aa_odd_face_fp64(a, t, s);
     g->iteration += 2;
   }
@@ -1222,6 +1333,7 @@ int lbm_aa_slab_even_part(KernelData* kd, CaseData* cd, int part, void* stream) 
   Gpu* g = reinterpret_cast<Gpu*>(kd);
   if (part < 0 || part > 1 || (g->kind != kAa && !g->listSlab)) return -1;
   sync_upload(g);
+  if (refuse_lost(g)) return -4;
   const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
   const cudaStream_t s = stream_or(g, stream);
   if (g->listSlab) {
@@ -1230,7 +1342,7 @@ int lbm_aa_slab_even_part(KernelData* kd, CaseData* cd, int part, void* stream) 
     if (!split) {
       if (part == 1) {
         if (g->storage != lbm::kStoreF64)
-          lbm::list_even_lp(list_args_lp(g), to_float(t), g->storage, s);
+          lbm::list_even_lp(list_args_lp(g), to_trtw(t), g->storage, s);
         else
           lbm::list_even_fp64(list_args(g), t, s);
       }
@@ -1241,7 +1353,7 @@ int lbm_aa_slab_even_part(KernelData* kd, CaseData* cd, int part, void* stream) 
     for (int k = 0; k < 2; ++k) {
       if (r[k][1] <= r[k][0]) continue;
       if (g->storage != lbm::kStoreF64)
-        lbm::list_even_lp_tiles(list_args_lp(g), to_float(t), g->storage, r[k][0], r[k][1], s);
+        lbm::list_even_lp_tiles(list_args_lp(g), to_trtw(t), g->storage, r[k][0], r[k][1], s);
       else
         lbm::list_even_fp64_tiles(list_args(g), t, r[k][0], r[k][1], s);
     }
@@ -1264,6 +1376,7 @@ int lbm_aa_slab_odd_part(KernelData* kd, CaseData* cd, int part, void* stream) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
   if (part < 0 || part > 1 || (g->kind != kAa && !g->listSlab)) return -1;
   sync_upload(g);
+  if (refuse_lost(g)) return -4;
   const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
   const cudaStream_t s = stream_or(g, stream);
   if (g->listSlab) {
@@ -1287,7 +1400,7 @@ int lbm_aa_slab_odd_part(KernelData* kd, CaseData* cd, int part, void* stream) {
       const int t0 = r[k][0], t1 = r[k][1];
       if (t1 <= t0) continue;
       if (g->storage != lbm::kStoreF64)
-        lbm::list_odd_lp_tiles(list_args_lp(g), to_float(t), g->storage, t0, t1, s);
+        lbm::list_odd_lp_tiles(list_args_lp(g), to_trtw(t), g->storage, t0, t1, s);
       else
         lbm::list_odd_fp64_tiles(list_args(g), t, t0, t1, s);
     }
@@ -1295,8 +1408,7 @@ int lbm_aa_slab_odd_part(KernelData* kd, CaseData* cd, int part, void* stream) {
     const lbm::AaArgs a = aa_args(g);
     if (part == 0) {
       // the interior blocks read and write only the slab's own planes
-      if (g->nDirect > 0) lbm::aa_odd_interior_fp64(a, t, g->dOddBlocks, g->nDirect, 0, s);
-      if (g->nGeneral > 0) lbm::aa_odd_interior_fp64(a, t, g->dOddBlocks + g->nDirect, 0, g->nGeneral, s);
+      if (g->nOddItems > 0) lbm::aa_odd_interior_fp64(a, t, g->dOddItems, g->nOddItems, g->dOddCells, s);
     } else if (lbm::aa_shell_cells(a) > 0) {
       lbm::aa_odd_face_fp64(a, t, s);
     }
@@ -1312,6 +1424,7 @@ int lbm_b200_checkpoint_save(KernelData* kd, const char* path) {
   }
   cudaError_t e = cudaStreamSynchronize(g->stream);
   if (e != cudaSuccess) { g_lastError = cudaGetErrorString(e); return (int)e; }
+  if (g->stateLost || read_device_error(g)) return -4;
   download(g);
   CkptHeader h = ckpt_header_of(g);
   const size_t bytes = g->mirrorElems * g->elemBytes;
@@ -1335,11 +1448,11 @@ int lbm_b200_checkpoint_load(KernelData* kd, const char* path) {
     return -2;
   }
   bool same = h.kind == want.kind && h.storage == want.storage && h.nFluid == want.nFluid && h.elems == want.elems &&
-              h.elemBytes == want.elemBytes && h.lambda == want.lambda;
+              h.elemBytes == want.elemBytes && h.lambda == want.lambda && h.maskHash == want.maskHash;
   for (int i = 0; i < 3; ++i) same = same && h.dims[i] == want.dims[i] && h.per[i] == want.per[i];
   if (!same) {
     std::fclose(fh);
-    g_lastError = std::string(path) + " was written by an instance of another kernel, lattice, storage or Lambda";
+    g_lastError = std::string(path) + " was written by an instance of another kernel, lattice (geometry), storage or Lambda";
     return -2;
   }
   cudaError_t e = cudaStreamSynchronize(g->stream);
@@ -1363,6 +1476,7 @@ int lbm_b200_checkpoint_load(KernelData* kd, const char* path) {
   if (g->storage != lbm::kStoreF64) raw_to_mirror(g);
   g->dirty = false;
   g->iteration = h.iteration;
+  clear_lost(g);
   return 0;
 }
 
@@ -1371,6 +1485,7 @@ void lbm_b200_mark_mirror_dirty(KernelData* kd) { reinterpret_cast<Gpu*>(kd)->di
 int lbm_b200_time_steps(KernelData* kd, CaseData* cd, int n, double* total_ms, double* per_launch_ms) {
   Gpu* g = reinterpret_cast<Gpu*>(kd);
   if (g->dirty) upload_if_dirty(g);
+  if (refuse_lost(g)) return -4;
   const lbm::Trt<double> t = make_trt(cd->Omega, g->lambda, cd->XForce);
   const long nl = launches_for(g, n);
   cudaEvent_t* ev = static_cast<cudaEvent_t*>(std::malloc(sizeof(cudaEvent_t) * (nl + 1)));
@@ -1394,9 +1509,7 @@ int lbm_b200_time_steps(KernelData* kd, CaseData* cd, int n, double* total_ms, d
   for (long k = 0; k <= nl; ++k) cudaEventDestroy(ev[k]);
   std::free(ev);
   if (e != cudaSuccess) { g_lastError = cudaGetErrorString(e); return (int)e; }
-  int err = 0;
-  cudaMemcpy(&err, g->dErr, sizeof(int), cudaMemcpyDeviceToHost);
-  if (err) { g_lastError = "a device wait exceeded its limit"; return -1; }
+  if (read_device_error(g)) return -1;
   return 0;
 }
 
@@ -1432,11 +1545,13 @@ int lbm_b200_instance_moments(KernelData* kd, double* out) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
     if (e == cudaSuccess) e = cudaMemcpy(out, g->dMomOut, 4 * sizeof(double), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) g_lastError = cudaGetErrorString(e);
+    if (e == cudaSuccess && (g->stateLost || read_device_error(g))) return -4;  // sums of a lost state
     return (int)e;
   }
   int rc = lbm_b200_moments_device(current_grid(g), g->nCells, g->nFluid, g->dMomOut, g->stream);
   if (rc) return rc;
   cudaError_t e = cudaMemcpy(out, g->dMomOut, 4 * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && (g->stateLost || read_device_error(g))) return -4;  // sums of a lost state
   return (int)e;
 }
 

@@ -579,10 +579,43 @@ static double x_velocity(const double *p)
 	return p[dE] + p[dNE] + p[dSE] + p[dTE] + p[dBE] - p[dW] - p[dNW] - p[dSW] - p[dTW] - p[dBW];
 }
 
+/* The profile error of an x-velocity slice (slice[y * nz + z]) and, with
+ * write_file, the reference's flow-profile.dat (src/Kernel.c:547-616). */
+double lbmh_verify_profile(int ny, int nz, double omega, double xforce, const double *slice, int write_file)
+{
+	const double visc = (1.0 / omega - 0.5) / 3.0;
+	const int evenNy = ny % 2 == 0;
+	const int ym = (ny - evenNy - 1) / 2;
+	const double center = ny / 2.0;
+	const double rmax = (double)ny / 2.0 - 1.0;
+	const double r2max = rmax * rmax;
+	const double umax = xforce * r2max / (2.0 * visc);
+
+	FILE *fh = NULL;
+	if (write_file) {
+		fh = fopen("flow-profile.dat", "w");
+		if (fh) fprintf(fh, "# z coord., radius, analytic, simulation, diff abs, diff rel, undim_analytic, undim_sim\n");
+	}
+	double dev = 0.0;
+	for (int z = 0; z < nz; ++z) {
+		const double r = z - center + 0.5;
+		const double r2 = r * r;
+		const double ua = r2 >= r2max ? 0.0 : xforce * (r2max - r2) / (2.0 * visc);
+		const double us = evenNy ? (slice[ym * nz + z] + slice[(ym + 1) * nz + z]) / 2.0 : slice[ym * nz + z];
+		double rel = 0.0;
+		if (ua != 0.0) {
+			rel = fabs(ua - us) / ua;
+			dev += rel * rel;
+		}
+		if (fh) fprintf(fh, "%d\t%e\t%e\t%e\t%e\t%e\t%e\t%e\n", z, r / center, ua, us, fabs(ua - us), rel, ua / umax, us / umax);
+	}
+	if (fh) fclose(fh);
+	return sqrt(dev);
+}
+
 double lbm_verify(LatticeDesc *ld, KernelData *kd, CaseData *cd, int write_file)
 {
 	const int nx = ld->Dims[0], ny = ld->Dims[1], nz = ld->Dims[2];
-	const double visc = (1.0 / cd->Omega - 0.5) / 3.0;
 	const int xs = nx / 2;
 	double *slice = (double *)malloc(sizeof(double) * (size_t)ny * nz);
 	double p[19];
@@ -596,35 +629,9 @@ double lbm_verify(LatticeDesc *ld, KernelData *kd, CaseData *cd, int write_file)
 		}
 		slice[y * nz + z] = u;
 	}
-
-	const int evenNy = ny % 2 == 0;
-	const int ym = (ny - evenNy - 1) / 2;
-	const double center = ny / 2.0;
-	const double rmax = (double)ny / 2.0 - 1.0;
-	const double r2max = rmax * rmax;
-	const double umax = cd->XForce * r2max / (2.0 * visc);
-
-	FILE *fh = NULL;
-	if (write_file) {
-		fh = fopen("flow-profile.dat", "w");
-		if (fh) fprintf(fh, "# z coord., radius, analytic, simulation, diff abs, diff rel, undim_analytic, undim_sim\n");
-	}
-	double dev = 0.0;
-	for (int z = 0; z < nz; ++z) {
-		const double r = z - center + 0.5;
-		const double r2 = r * r;
-		const double ua = r2 >= r2max ? 0.0 : cd->XForce * (r2max - r2) / (2.0 * visc);
-		const double us = evenNy ? (slice[ym * nz + z] + slice[(ym + 1) * nz + z]) / 2.0 : slice[ym * nz + z];
-		double rel = 0.0;
-		if (ua != 0.0) {
-			rel = fabs(ua - us) / ua;
-			dev += rel * rel;
-		}
-		if (fh) fprintf(fh, "%d\t%e\t%e\t%e\t%e\t%e\t%e\t%e\n", z, r / center, ua, us, fabs(ua - us), rel, ua / umax, us / umax);
-	}
-	if (fh) fclose(fh);
+	const double err = lbmh_verify_profile(ny, nz, cd->Omega, cd->XForce, slice, write_file);
 	free(slice);
-	return sqrt(dev);
+	return err;
 }
 
 /* ------------------------------------------------------------------------ */

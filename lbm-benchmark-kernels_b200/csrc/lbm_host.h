@@ -78,6 +78,11 @@ void lbmh_aa_links(const LatticeDesc *ld, int xs, int pitch, int zoff, uint32_t 
 void lbmh_aa_links_range(const LatticeDesc *ld, int x0, int x1, int xs, int pitch, int zoff, uint32_t *link);
 
 /* IEEE binary16 <-> binary32 (round to nearest even). */
+/* Profile error of an x-velocity slice (nY x nZ, slice[y * nz + z]) against
+ * the analytic channel profile, and with write_file the reference's
+ * flow-profile.dat (src/Kernel.c:547-616). */
+double lbmh_verify_profile(int ny, int nz, double omega, double xforce, const double *slice, int write_file);
+
 float lbmh_f16_to_f32(uint16_t h);
 uint16_t lbmh_f32_to_f16(float f);
 

@@ -4,6 +4,7 @@
 #include <atomic>
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -158,8 +159,8 @@ int list_runs_device(const uint32_t* adj, int nFluid, cudaStream_t s, uint32_t**
                      size_t* runBytes);
 
 // Launchers (stream-ordered, no synchronisation).
-void list_even_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s);
-void list_odd_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s);
+void list_even_lp(const ListArgsLp& a, const TrtW& t, int storage, cudaStream_t s);
+void list_odd_lp(const ListArgsLp& a, const TrtW& t, int storage, cudaStream_t s);
 // The odd steps over tiles [t0, t1) only (slabs overlap their halo exchange
 // with the tiles that read no ghost node).
 void list_odd_fp64_tiles(const ListArgs& a, const Trt<double>& t, int t0, int t1, cudaStream_t s);
@@ -167,21 +168,22 @@ void list_odd_fp64_tiles(const ListArgs& a, const Trt<double>& t, int t0, int t1
 // also for FP16, whose whole-array step is the staged kernel) and the
 // full-array even step over x planes [x0, x1).
 void list_even_fp64_tiles(const ListArgs& a, const Trt<double>& t, int t0, int t1, cudaStream_t s);
-void list_even_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int storage, int t0, int t1, cudaStream_t s);
+void list_even_lp_tiles(const ListArgsLp& a, const TrtW& t, int storage, int t0, int t1, cudaStream_t s);
 void aa_even_fp64_planes(const AaArgs& a, const Trt<double>& t, int x0, int x1, cudaStream_t s);
-void list_odd_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int storage, int t0, int t1, cudaStream_t s);
+void list_odd_lp_tiles(const ListArgsLp& a, const TrtW& t, int storage, int t0, int t1, cudaStream_t s);
 void aa_even_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
-// The AA odd step: the interior blocks (a list of nDirect blocks for the
-// direct kernel, followed by nGeneral blocks for the general one, built by
-// aa_interior_blocks), then the face shell.
-void aa_odd_interior_fp64(const AaArgs& a, const Trt<double>& t, const int* blocks, int nDirect, int nGeneral,
+// The AA odd step: the interior launch over a list of work items (built by
+// aa_interior_items), then the face shell.
+void aa_odd_interior_fp64(const AaArgs& a, const Trt<double>& t, const int* items, int nItems, const int* cells,
                           cudaStream_t s);
-// Host: sorts the interior blocks of the odd step by the link words of their
-// cells (link: the host copy of the device link array). Fills `blocks` (room
-// for aa_interior_block_count entries) with the direct blocks, then the
-// general ones; blocks without fluid cells are left out.
+// Host: the interior work items of the odd step from the link words (link:
+// the host copy of the device link array), in x-plane order. Per plane:
+// the ids of the interior blocks that hold at least one direct fluid cell
+// (no reversed link), then one item ~k per chunk k of 128 entries of `cells`
+// (the cell indices of the plane's interior fluid cells with a reversed
+// link, ascending, the last chunk padded with -1).
 long long aa_interior_block_count(const AaArgs& a);
-void aa_interior_blocks(const AaArgs& a, const uint32_t* link, int* blocks, int* nDirect, int* nGeneral);
+void aa_interior_items(const AaArgs& a, const uint32_t* link, std::vector<int>& items, std::vector<int>& cells);
 void aa_odd_face_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
 bool aa_has_interior(const AaArgs& a);
 // Two-grid full-array push / pull steps (push-soa / pull-soa): every fluid
@@ -193,6 +195,20 @@ void list_even_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
 void list_odd_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
 void list_pull_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
 void list_push_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
+
+// The -verify check on the device (lbm_verify.cu). A slice cell i = y * nZ +
+// z at x = nX/2 reads PDF d at element base[i] + off[d] of f (storage
+// kStoreF64/F32/F16); base[i] < 0 marks an obstacle. Writes the x-velocity
+// slice (nY * nZ doubles) and err[0] = the Poiseuille error norm.
+struct VerifyArgs {
+  const void* f;
+  int storage;
+  const long long* base;
+  long long off[Q];
+  int nY, nZ;
+  double xforce, visc;
+};
+void verify_device(const VerifyArgs& a, double* slice, double* err, cudaStream_t s);
 
 // FP64 mass and momentum sums of a list-layout field (lbm_moments.cu):
 // pass 1 writes 4 partial sums per block of kListTile nodes into `partials`

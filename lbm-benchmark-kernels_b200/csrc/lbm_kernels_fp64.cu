@@ -88,22 +88,31 @@ __global__ void __launch_bounds__(128, 8) k_aa_even_fp64(const AaArgs a, const T
 // (x + c_i, i) with the increment of i, or -- bounced back at a wall -- to
 // its own slot (x, inv(i)) with the increment of inv(i).
 //
-// Three launches share the step. The interior kernels take every cell off
-// the x and y faces -- and off the z faces too unless z is periodic: links of
+// Two launches share the step. The interior launch takes every cell off the
+// x and y faces -- and off the z faces too unless z is periodic: links of
 // these cells leave the domain at most through a periodic z face, which is a
-// fixed offset of -/+ nZ cells. Their blocks (32 z-cells x 4 y-rows of one x
-// plane) are sorted on the host into two lists: blocks whose fluid cells have
-// no reversed link run the direct kernel, where every address is the
-// neighbour's slot; the others run the general kernel, where each address is
-// a select between the neighbour's slot and the node's own slot. Blocks
-// without fluid cells are not launched. In both, the 19 loads are issued
-// together. The face kernel takes the remaining shell: links that leave the
-// domain wrap periodically on every crossed axis, or, at a non-periodic face,
-// go to the ghost layer (an "open" link), as in the reference.
+// fixed offset of -/+ nZ cells. Interior cells are sorted on the host by
+// their link words: a cell without reversed links is "direct" (every address
+// is the neighbour's slot), the others are "general" (each address is a
+// select between the neighbour's slot and the node's own slot). The launch
+// runs a list of work items in x-plane order: for each plane, the blocks
+// (32 z-cells x 4 y-rows) that hold at least one direct cell -- these skip
+// the general cells in them -- then chunks of 128 of the plane's general
+// cells, one thread per cell. So the select-free path covers every direct
+// cell, also those next to a wall (in a 256^3 channel a split by whole blocks
+// sends 27 % of the cells, every block with one wall-adjacent cell, down the
+// general path; the general cells are 1.6 %), and a general cell runs while
+// the direct blocks of its plane touch the same 32-byte sectors, so its
+// scattered accesses (a column of wall-adjacent cells is `pitch` apart) hit
+// L2 instead of DRAM. Blocks without fluid cells are not launched. In both
+// paths the 19 loads are issued together. The face kernel takes the
+// remaining shell: links that leave the domain wrap periodically on every
+// crossed axis, or, at a non-periodic face, go to the ghost layer (an "open"
+// link), as in the reference.
 //
 // Cells of different nodes never share a slot in the odd step (each node
-// reads and writes only its own links' slots), so the three launches may run
-// in any order.
+// reads and writes only its own links' slots), so the work items and the
+// two launches may run in any order.
 
 // Interior block `id` of the list: (bz, by, bx) with bz fastest.
 __device__ __forceinline__ void aa_interior_block(const AaArgs& a, int id, int& z, int& y, int& x) {
@@ -115,33 +124,23 @@ __device__ __forceinline__ void aa_interior_block(const AaArgs& a, int id, int& 
   x = 1 + rest / gy;
 }
 
-// Launch bounds: the direct kernel is capped at 7 resident blocks of 128
-// threads per SM (68 registers, no spills), the general one at 5 (96); both
-// measured fastest among 1-8 on B200. Addresses are the cell's base pointer
-// plus a per-direction offset from the parameter bank (and the z wrap), so no
-// per-direction address stays live in registers.
-template <bool kDirect>
-__global__ void __launch_bounds__(128, kDirect ? 7 : 5)
-    k_aa_odd_interior_fp64(const AaArgs a, const Trt<double> t, const int* blocks) {
-  int x, y, z;
-  aa_interior_block(a, blocks[blockIdx.x], z, y, x);
-  const int zHi = a.perZ ? a.nZ - 1 : a.nZ - 2;
-  if (z > zHi || y > a.nY - 2) return;
-  const int c = aa_cell(a, x, y, z);
+// The periodic z wrap of an interior cell, decided once per cell: a link
+// with c_z = -1 leaving through z = 0 moves +nZ cells, one with c_z = +1
+// through z = nZ-1 moves -nZ (only reachable when z is periodic: otherwise
+// interior cells are off the z faces).
+struct ZWrap {
+  int down, up;
+  __device__ __forceinline__ ZWrap(const AaArgs& a, int z)
+      : down(z == 0 ? a.nZ : 0), up(z == a.nZ - 1 ? -a.nZ : 0) {}
+  __device__ __forceinline__ int operator()(int d) const { return cz(d) < 0 ? down : (cz(d) > 0 ? up : 0); }
+};
+
+// A general cell (interior, fluid, at least one reversed link).
+__device__ __noinline__ void aa_odd_general_cell(const AaArgs& a, const Trt<double>& t, int c) {
+  const int z = c % a.pitch - kZOff;  // a row is `pitch` cells; interior z = 0 sits at kZOff
   const uint32_t w = __ldg(a.link + c);
-  if (!(w & kFluidBit)) return;
   double* const fb = a.f + c;
-  // the periodic z wrap, decided once per cell: a link with c_z = -1 leaving
-  // through z = 0 moves +nZ cells, one with c_z = +1 through z = nZ-1 moves -nZ
-  const int wrapDown = z == 0 ? a.nZ : 0, wrapUp = z == a.nZ - 1 ? -a.nZ : 0;
-  auto wrap = [&](int d) -> int { return cz(d) < 0 ? wrapDown : (cz(d) > 0 ? wrapUp : 0); };
-  if (kDirect) {
-    // store addresses come from a laundered base pointer, apart from the load
-    // addresses, so those need not stay live across the collision
-    trt_update(t, [&](int d) -> double { return fb[a.ldOff[d] + wrap(inv(d))] + t.force[d]; },
-               [&](int d, double v) { launder(fb)[a.stOff[d] + wrap(d)] = v + t.force[d]; });
-    return;
-  }
+  const ZWrap wrap(a, z);
   const int S = (int)a.dstride;
   auto load = [&](int d) -> double {
     if (d == DC) return fb[a.ldOff[DC]] + t.force[DC];
@@ -160,6 +159,37 @@ __global__ void __launch_bounds__(128, kDirect ? 7 : 5)
     fs[rev ? j * S : a.stOff[d] + wrap(d)] = v + (rev ? t.force[j] : t.force[d]);
   };
   trt_update(t, load, store);
+}
+
+// Work item `items[blockIdx.x]`: >= 0 a block id (direct cells), < 0 the
+// general-cell chunk ~item (cells[128 * chunk + thread], -1 = none).
+// Launch bounds: 7 resident blocks of 128 threads per SM (the direct path
+// takes 68 registers, no spills; measured fastest among 1-8 on B200; the
+// general path spills a few values into L1 under that cap). Direct addresses
+// are the cell's base pointer plus a per-direction offset from the parameter
+// bank (and the z wrap), so no per-direction address stays live in
+// registers; store addresses come from a laundered base pointer, apart from
+// the load addresses, so those need not stay live across the collision.
+__global__ void __launch_bounds__(128, 7)
+    k_aa_odd_interior_fp64(const __grid_constant__ AaArgs a, const __grid_constant__ Trt<double> t, const int* items,
+                           const int* cells) {
+  const int item = __ldg(items + blockIdx.x);
+  if (item < 0) {
+    const int c = __ldg(cells + (size_t)(~item) * 128 + threadIdx.y * 32 + threadIdx.x);
+    if (c >= 0) aa_odd_general_cell(a, t, c);
+    return;
+  }
+  int x, y, z;
+  aa_interior_block(a, item, z, y, x);
+  const int zHi = a.perZ ? a.nZ - 1 : a.nZ - 2;
+  if (z > zHi || y > a.nY - 2) return;
+  const int c = aa_cell(a, x, y, z);
+  const uint32_t w = __ldg(a.link + c);
+  if ((w & (kFluidBit | kLinkBits)) != kFluidBit) return;  // solid, or a general cell (own item)
+  double* const fb = a.f + c;
+  const ZWrap wrap(a, z);
+  trt_update(t, [&](int d) -> double { return fb[a.ldOff[d] + wrap(inv(d))] + t.force[d]; },
+             [&](int d, double v) { launder(fb)[a.stOff[d] + wrap(d)] = v + t.force[d]; });
 }
 
 // Cell of shell index i: the x faces (all y, z), then the y faces (inner x,
@@ -414,35 +444,41 @@ long long aa_interior_block_count(const AaArgs& a) {
   return (nz + 31) / 32 * ((a.nY - 2 + 3) / 4) * (long long)(a.nX - 2);
 }
 
-void aa_interior_blocks(const AaArgs& a, const uint32_t* link, int* blocks, int* nDirect, int* nGeneral) {
-  *nDirect = *nGeneral = 0;
+void aa_interior_items(const AaArgs& a, const uint32_t* link, std::vector<int>& items, std::vector<int>& cells) {
+  items.clear();
+  cells.clear();
   const long long n = aa_interior_block_count(a);
   if (n == 0) return;
   const int zLo = a.perZ ? 0 : 1, zHi = a.perZ ? a.nZ - 1 : a.nZ - 2;
   const int gz = (zHi - zLo + 1 + 31) / 32, gy = (a.nY - 2 + 3) / 4;
-  std::vector<int> general;
-  for (long long id = 0; id < n; ++id) {
-    const int bz = (int)(id % gz), by = (int)(id / gz % gy), bx = (int)(id / gz / gy);
-    bool fluid = false, reversed = false;
-    for (int ty = 0; ty < 4; ++ty) {
-      const int y = 1 + by * 4 + ty;
-      if (y > a.nY - 2) break;
-      for (int tz = 0; tz < 32; ++tz) {
-        const int z = zLo + bz * 32 + tz;
-        if (z > zHi) break;
-        const uint32_t w = link[(long long)(bx + 2) * a.xs + (long long)(y + 1) * a.pitch + z + kZOff];
-        if (!(w & kFluidBit)) continue;
-        fluid = true;
-        reversed = reversed || (w & kLinkBits) != 0;
+  const long long perPlane = (long long)gz * gy;
+  auto word = [&](int x, int y, int z) { return link[(long long)(x + 1) * a.xs + (long long)(y + 1) * a.pitch + z + kZOff]; };
+  for (int x = 1; x <= a.nX - 2; ++x) {
+    // the plane's blocks holding direct cells (block ids: bz fastest, then by, then x)
+    for (long long k = 0; k < perPlane; ++k) {
+      const int bz = (int)(k % gz), by = (int)(k / gz);
+      bool direct = false;
+      for (int ty = 0; ty < 4 && !direct; ++ty) {
+        const int y = 1 + by * 4 + ty;
+        if (y > a.nY - 2) break;
+        for (int tz = 0; tz < 32; ++tz) {
+          const int z = zLo + bz * 32 + tz;
+          if (z > zHi) break;
+          if ((word(x, y, z) & (kFluidBit | kLinkBits)) == kFluidBit) { direct = true; break; }
+        }
       }
+      if (direct) items.push_back((int)((x - 1) * perPlane + k));
     }
-    if (!fluid) continue;
-    if (reversed)
-      general.push_back((int)id);
-    else
-      blocks[(*nDirect)++] = (int)id;
+    // then the plane's general cells in chunks of 128
+    const size_t first = cells.size();
+    for (int y = 1; y <= a.nY - 2; ++y)
+      for (int z = zLo; z <= zHi; ++z) {
+        const uint32_t w = word(x, y, z);
+        if ((w & kFluidBit) && (w & kLinkBits)) cells.push_back((x + 1) * a.xs + (y + 1) * a.pitch + z + kZOff);
+      }
+    while ((cells.size() - first) % 128) cells.push_back(-1);
+    for (size_t c = first; c < cells.size(); c += 128) items.push_back(~(int)(c / 128));
   }
-  for (int id : general) blocks[*nDirect + (*nGeneral)++] = id;
 }
 
 void aa_even_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
@@ -458,10 +494,9 @@ void aa_even_fp64_planes(const AaArgs& a, const Trt<double>& t, int x0, int x1, 
   k_aa_even_fp64<<<dim3((a.nZ + 127) / 128, a.nY, x1 - x0), 128, 0, s>>>(b, t);
 }
 
-void aa_odd_interior_fp64(const AaArgs& a, const Trt<double>& t, const int* blocks, int nDirect, int nGeneral,
+void aa_odd_interior_fp64(const AaArgs& a, const Trt<double>& t, const int* items, int nItems, const int* cells,
                           cudaStream_t s) {
-  if (nDirect > 0) k_aa_odd_interior_fp64<true><<<nDirect, dim3(32, 4), 0, s>>>(a, t, blocks);
-  if (nGeneral > 0) k_aa_odd_interior_fp64<false><<<nGeneral, dim3(32, 4), 0, s>>>(a, t, blocks + nDirect);
+  if (nItems > 0) k_aa_odd_interior_fp64<<<nItems, dim3(32, 4), 0, s>>>(a, t, items, cells);
 }
 
 void aa_odd_face_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {

@@ -12,15 +12,10 @@
 namespace lbm {
 
 template <class St>
-__global__ void __launch_bounds__(kListTile) k_list_even_lp(const ListArgsLp a, const Trt<float> t) {
-  using T = typename St::T;
+__global__ void __launch_bounds__(kListTile) k_list_even_lp(const ListArgsLp a, const TrtW w) {
   const int n = (blockIdx.x + a.tileBase) * kListTile + threadIdx.x;
   if (n >= a.nFluid) return;
-  T* const f = static_cast<T*>(a.f) + n;
-  T* const fs = launder(f);
-  const long long S = a.nCells;
-  trt_update(t, [&](int d) { return St::dev(f[d * S], d); },
-             [&](int d, float v) { fs[inv(d) * S] = St::raw(v, inv(d)); });
+  lp_even_node<St>(static_cast<typename St::T*>(a.f), a.nCells, n, TrtDev<St>(w));
 }
 
 // Even step with the PDF planes staged through shared memory by bulk copies
@@ -32,8 +27,9 @@ __global__ void __launch_bounds__(kListTile) k_list_even_lp(const ListArgsLp a, 
 // plane stride nCells to be a multiple of TN (the reduced-storage layout pads
 // it to whole kLpTileNodes tiles).
 template <class St, int StageBytes, int Stages>
-__global__ void __launch_bounds__(256) k_list_even_staged(const ListArgsLp a, const Trt<float> t) {
+__global__ void __launch_bounds__(256, 2) k_list_even_staged(const ListArgsLp a, const TrtW w) {
   using T = typename St::T;
+  const TrtDev<St> t(w);
   constexpr int TN = StageBytes / (int)sizeof(T);
   constexpr int NPT = TN / 256;
   static_assert(TN % 256 == 0 && StageBytes % 16 == 0, "stage layout");
@@ -85,19 +81,16 @@ __global__ void __launch_bounds__(256) k_list_even_staged(const ListArgsLp a, co
         float fa[Q], fb[Q], oa[Q], ob[Q];
 #pragma unroll
         for (int d = 0; d < Q; ++d) {
-          const float2 v = __half22float2(*reinterpret_cast<const __half2*>(buf + d * TN + local));
-          const float inv_s = 1.0f / StoreF16::scale(d);
-          fa[d] = v.x * inv_s;
-          fb[d] = v.y * inv_s;
+          const float2 v = StoreF16::in2(*reinterpret_cast<const __half2*>(buf + d * TN + local), d);
+          fa[d] = v.x;
+          fb[d] = v.y;
         }
-        trt_collide(t, fa, oa);
-        trt_collide(t, fb, ob);
+        trt_collide_dev(t, fa, oa);
+        trt_collide_dev(t, fb, ob);
         T* const fs = launder(f + n);
 #pragma unroll
-        for (int d = 0; d < Q; ++d) {
-          const float sc = StoreF16::scale(inv(d));
-          *reinterpret_cast<__half2*>(fs + inv(d) * S) = __floats2half2_rn(oa[d] * sc, ob[d] * sc);
-        }
+        for (int d = 0; d < Q; ++d)
+          *reinterpret_cast<__half2*>(fs + inv(d) * S) = StoreF16::out2(oa[d], ob[d], inv(d));
       }
     } else {
 #pragma unroll 1
@@ -106,16 +99,19 @@ __global__ void __launch_bounds__(256) k_list_even_staged(const ListArgsLp a, co
         const int n = tile * TN + local;
         if (n >= a.nFluid) break;
         T* const fs = launder(f + n);
-        trt_update(t, [&](int d) { return St::dev(buf[d * TN + local], d); },
-                   [&](int d, float v) { fs[inv(d) * S] = St::raw(v, inv(d)); });
+        float x[Q], o[Q];
+#pragma unroll
+        for (int d = 0; d < Q; ++d) x[d] = St::in(buf[d * TN + local], d);
+        trt_collide_dev(t, x, o);
+#pragma unroll
+        for (int d = 0; d < Q; ++d) fs[inv(d) * S] = St::out(o[d], inv(d));
       }
     }
   }
 }
 
 template <class St>
-__global__ void __launch_bounds__(kListTile) k_list_odd_lp(const ListArgsLp a, const Trt<float> t) {
-  using T = typename St::T;
+__global__ void __launch_bounds__(kListTile, 6) k_list_odd_lp(const ListArgsLp a, const TrtW w) {
   __shared__ alignas(128) uint32_t srun[kRunTileWords];
   __shared__ alignas(8) uint64_t bar;
   __shared__ int ok;
@@ -124,22 +120,7 @@ __global__ void __launch_bounds__(kListTile) k_list_odd_lp(const ListArgsLp a, c
   if (n >= a.nFluid) return;
   uint32_t off;
   const uint32_t* e = run_row(srun, threadIdx.x, off);  // link d = e[d] + off (run-compressed adjacency)
-  T* const f = static_cast<T*>(a.f);
-  const long long S = a.nCells;
-  auto load = [&](int d) -> float {
-    return St::dev(d == DC ? f[DC * S + n] : f[e[inv(d)] + off], d) + t.force[d];
-  };
-  auto store = [&](int d, float v) {
-    if (d == DC) {
-      f[DC * S + n] = St::raw(v + t.force[DC], DC);
-      return;
-    }
-    const uint32_t dst = reinterpret_cast<const volatile uint32_t*>(e)[d] + off;  // re-read: keeps no 64-bit addresses live across the collision
-    const int j = inv(d);
-    const bool bounce = dst == static_cast<uint32_t>(j * S + n);
-    f[dst] = St::raw(v + (bounce ? t.force[j] : t.force[d]), d);  // the scale is equal for d and inv(d)
-  };
-  trt_update(t, load, store);
+  lp_odd_node<St>(static_cast<typename St::T*>(a.f), static_cast<uint32_t>(a.nCells), n, e, off, TrtDev<St>(w));
 }
 
 static unsigned lp_blocks(const ListArgsLp& a) { return (a.nFluid + kListTile - 1) / kListTile; }
@@ -151,7 +132,7 @@ constexpr int kEvenStageBytes = 2048, kEvenStages = 2, kEvenBlocksPerSM = 2;
 // The kernel's shared-memory opt-in is a per-device attribute: it is set once
 // per device (and per storage type), with the grid sized to that device.
 template <class St>
-static void launch_even_staged(const ListArgsLp& a, const Trt<float>& t, cudaStream_t s) {
+static void launch_even_staged(const ListArgsLp& a, const TrtW& t, cudaStream_t s) {
   constexpr int kMaxDevices = 64;
   static std::atomic<int> grid[kMaxDevices];
   constexpr size_t smem = (size_t)kEvenStages * Q * kEvenStageBytes;
@@ -173,7 +154,7 @@ static void launch_even_staged(const ListArgsLp& a, const Trt<float>& t, cudaStr
 // FP16: the staged even step (0.118 -> 0.100 ms at 6.7M nodes on B200, 66 ->
 // 78 % of the measured HBM bandwidth). FP32: the direct kernel, whose 4-byte
 // loads already keep enough bytes in flight (0.162 ms direct, 0.174 staged).
-void list_even_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s) {
+void list_even_lp(const ListArgsLp& a, const TrtW& t, int storage, cudaStream_t s) {
   if (a.nFluid <= 0) return;
   ListArgsLp b = a;
   b.tileBase = 0;
@@ -185,7 +166,7 @@ void list_even_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStr
 
 // Tile ranges run the per-node kernel for both storages (the FP16 staged
 // kernel works on whole 1024-node tiles).
-void list_even_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int storage, int t0, int t1, cudaStream_t s) {
+void list_even_lp_tiles(const ListArgsLp& a, const TrtW& t, int storage, int t0, int t1, cudaStream_t s) {
   if (a.nFluid <= 0 || t1 <= t0) return;
   ListArgsLp b = a;
   b.tileBase = t0;
@@ -197,7 +178,7 @@ void list_even_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int storage, i
 
 static std::atomic<int> ahead16{0}, ahead32{0};
 
-void list_odd_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int storage, int t0, int t1, cudaStream_t s) {
+void list_odd_lp_tiles(const ListArgsLp& a, const TrtW& t, int storage, int t0, int t1, cudaStream_t s) {
   if (a.nFluid <= 0 || t1 <= t0) return;
   ListArgsLp b = a;
   b.tileBase = t0;
@@ -210,7 +191,7 @@ void list_odd_lp_tiles(const ListArgsLp& a, const Trt<float>& t, int storage, in
   }
 }
 
-void list_odd_lp(const ListArgsLp& a, const Trt<float>& t, int storage, cudaStream_t s) {
+void list_odd_lp(const ListArgsLp& a, const TrtW& t, int storage, cudaStream_t s) {
   if (a.nFluid <= 0) return;
   ListArgsLp b = a;
   b.tileBase = 0;

@@ -21,7 +21,9 @@
 // In host code `g_moment_scratch` names a host-side shadow, not device memory;
 // a kernel given that name would fault or read the wrong memory. The device
 // address is obtained with cudaGetSymbolAddress, once per device, with that
-// device current, on the first call of the entry point on that device.
+// device current, on the first call of the entry point on that device, and
+// kept for the life of the process: the cache assumes the device's context is
+// not reset (cudaDeviceReset) while the process uses this entry point.
 #include <cstdio>
 #include <mutex>
 
@@ -81,6 +83,14 @@ int lbm_b200_moments_noalloc(const double* pdfs, long long nCells, int nFluid, d
                  "(at most %lld nodes); use lbm_b200_moments_device instead\n",
                  nFluid, lbm::kNoAllocMaxNodes);
     return -2;
+  }
+  // an error left by earlier, unrelated work is reported as such, not as
+  // this call's: the call refuses to enqueue behind it
+  cudaError_t before = cudaPeekAtLastError();
+  if (before != cudaSuccess) {
+    std::fprintf(stderr, "lbm_b200_moments_noalloc: an earlier CUDA error is pending (%s); nothing enqueued\n",
+                 cudaGetErrorString(before));
+    return (int)before;
   }
   double* scratch = nullptr;
   int rc = scratch_on_current_device(&scratch);

@@ -291,7 +291,18 @@ class Instance:
                                  pdfs.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
 
     def verify(self, cd, write_file=False):
+        """KernelVerifiy through GetNode on the host mirror (lbm_verify)."""
         return lib().lbm_verify(ctypes.byref(self.lattice.desc), self.kdp, ctypes.byref(cd), int(write_file))
+
+    def verify_device(self, cd, write_file=False):
+        """The same check on the device (lbm_b200_verify_device): only the
+        x-velocity slice and the error come back to the host."""
+        err = ctypes.c_double(0.0)
+        rc = lib().lbm_b200_verify_device(ctypes.byref(self.lattice.desc), self.kdp, ctypes.byref(cd),
+                                          int(write_file), ctypes.byref(err))
+        if rc:
+            raise RuntimeError("device verify failed (%d): %s" % (rc, lib().lbm_b200_last_error().decode()))
+        return err.value
 
     def density(self):
         return lib().lbm_density(self.kdp, ctypes.byref(self.lattice.desc))

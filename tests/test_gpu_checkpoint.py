@@ -89,3 +89,62 @@ def test_batch_domain_restart(tmp_path):
         assert np.array_equal(got[m], want[m])
     finally:
         b.close()
+
+
+def test_checkpoint_of_another_geometry_with_equal_counts_is_refused(tmp_path):
+    # two masks with the same dimensions, periodicity and fluid count that
+    # differ in where one obstacle cell sits: the lattice hash tells them apart
+    dims = (10, 8, 9)
+    m1 = np.ones(int(np.prod(dims)), dtype=np.int32)
+    m2 = m1.copy()
+    m1[123] = 0
+    m2[321] = 0
+    a = lbmb200.kernel("cuda-list-aa-pv-soa").init(lbmb200.Lattice(m1, dims, (1, 1, 1)))
+    b = lbmb200.kernel("cuda-list-aa-pv-soa").init(lbmb200.Lattice(m2, dims, (1, 1, 1)))
+    try:
+        a.run(lbmb200.case(iterations=2))
+        a.checkpoint(str(tmp_path / "a.ckpt"))
+        with pytest.raises(RuntimeError, match=r"\(-2\)"):
+            b.restore(str(tmp_path / "a.ckpt"))
+        a.restore(str(tmp_path / "a.ckpt"))  # its own file still loads
+    finally:
+        a.deinit()
+        b.deinit()
+
+
+def test_lost_device_state_is_refused_until_a_state_is_uploaded():
+    # the error word a bounded wait sets when it gives up, written from the
+    # host (no kernel faults): steps, downloads and checkpoints refuse until
+    # set_field uploads a state again
+    import ctypes
+    L = lbmb200.lib()
+    lat = lbmb200.geometry("blocks-2", (14, 12, 10), (1, 0, 1))
+    init = random_pdfs(lat.mask.size, 31)
+    cd = lbmb200.case(omega=1.2, xforce=3e-5, iterations=4)
+    inst = lbmb200.kernel("cuda-list-aa-pv-soa").init(lat, kernel_args=["-lambda", "3/16"])
+    ref = lbmb200.kernel("cuda-list-aa-pv-soa").init(lat, kernel_args=["-lambda", "3/16"])
+    try:
+        inst.set_field(init)
+        inst.step_device(cd, 4)
+        inst.sync_mirror()
+        good = inst.get_field()
+        assert L.lbm_b200_inject_device_error(inst.kdp, 1) == 0
+        assert L.lbm_b200_sync_mirror(inst.kdp) == -4
+        m = lat.mask != 0
+        assert np.array_equal(inst.get_field()[m], good[m])  # the mirror keeps the last good state
+        assert L.lbm_b200_step_device(inst.kdp, ctypes.byref(cd), 2) == -4
+        tot = ctypes.c_double(0.0)
+        assert L.lbm_b200_time_steps(inst.kdp, ctypes.byref(cd), 2, ctypes.byref(tot), None) == -4
+        out = (ctypes.c_double * 4)()
+        assert L.lbm_b200_instance_moments(inst.kdp, out) == -4
+        # a state upload clears it: the run continues exactly as a clean instance
+        inst.set_field(init)
+        inst.step_device(cd, 4)
+        inst.sync_mirror()
+        ref.set_field(init)
+        ref.step_device(cd, 4)
+        ref.sync_mirror()
+        assert np.array_equal(inst.get_field()[m], ref.get_field()[m])
+    finally:
+        inst.deinit()
+        ref.deinit()

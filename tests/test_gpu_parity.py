@@ -200,3 +200,44 @@ def test_bounded_wait_reports_instead_of_hanging():
         inst.run(lbmb200.case(iterations=2))
     finally:
         inst.deinit()
+
+
+@pytest.mark.parametrize("kname", [k[0] for k in KERNELS])
+@pytest.mark.parametrize("lam,expect", [("1/12", "4.561374e-02"), ("3/16", "7.855978e-02")])
+def test_verify_on_device_known_answers(kname, lam, expect):
+    # the -verify preset run on the device only (no mirror download), then the
+    # slice and the error computed on the device: the reference's known answer
+    lat = lbmb200.geometry("box", (16, 16, 16), (1, 1, 0))
+    cd = lbmb200.case(omega=1.0, xforce=1e-5, iterations=1000)
+    inst = lbmb200.kernel(kname).init(lat, kernel_args=["-lambda", lam])
+    try:
+        inst.set_initial_density(cd)
+        inst.set_initial_velocity(cd)
+        inst.step_device(cd, 1000)
+        err = inst.verify_device(cd)
+        assert "%e" % err == expect
+        h2d, d2h = inst.last_copy_bytes()
+        assert d2h == 8 * (16 * 16 + 1)  # the slice and the error, not the field
+        inst.sync_mirror()
+        assert abs(inst.verify(cd) - err) <= 1e-15 * err  # the host check over the mirror agrees
+    finally:
+        inst.deinit()
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_verify_on_device_reduced_storage(prec):
+    # the reduced-storage forms: the device check reads the stored deviations
+    # exactly as the host mirror restores them
+    lat = lbmb200.geometry("box", (16, 16, 16), (1, 1, 0))
+    cd = lbmb200.case(omega=1.0, xforce=1e-5, iterations=1000)
+    inst = lbmb200.kernel("cuda-list-aa-pv-soa").init(lat, kernel_args=["-lambda", "3/16", "-precision", prec])
+    try:
+        inst.set_initial_density(cd)
+        inst.set_initial_velocity(cd)
+        inst.step_device(cd, 1000)
+        err = inst.verify_device(cd)
+        inst.sync_mirror()
+        assert abs(inst.verify(cd) - err) <= 1e-15 * err
+        assert abs(err - 7.855978e-02) < (1e-5 if prec == "fp32" else 1e-2)
+    finally:
+        inst.deinit()
