@@ -140,6 +140,11 @@ class Reference:
     def set_threads(self, n):
         return self.lib.refh_set_threads(int(n))
 
+    def pin(self, cpus):
+        """Pins the OpenMP threads to `cpus` (thread i to cpus[i]) with the
+        reference's own pinning code; returns the number of failures."""
+        return self.lib.refh_pin(",".join(str(int(c)) for c in cpus).encode())
+
     def kernels(self):
         return [self.lib.refh_kernel_name(i).decode() for i in range(self.lib.refh_kernel_count())]
 

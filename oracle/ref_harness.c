@@ -15,6 +15,7 @@
 #include "BenchKernelD3Q19ListAaCommon.h"
 #include "KernelFunctions.h"
 #include "Geometry.h"
+#include "Pinning.h"
 
 #include <malloc.h>
 #include <stdint.h>
@@ -45,6 +46,23 @@ int refh_set_threads(int n)
 	(void)n;
 	return 1;
 #endif
+}
+
+// Pins OpenMP thread i to the i-th CPU of cpuList ("0,2,4,..."), as the
+// reference's -pin does (src/Main.c:505-530, PinCurrentThreadByCpuList of
+// src/Pinning.c). Returns the number of threads whose pinning failed.
+int refh_pin(const char *cpuList)
+{
+	int failed = 0;
+#ifdef _OPENMP
+	#pragma omp parallel reduction(+:failed)
+	{
+		if (PinCurrentThreadByCpuList(cpuList, omp_get_thread_num()) != 0) failed += 1;
+	}
+#else
+	(void)cpuList;
+#endif
+	return failed;
 }
 
 // Builds a geometry with the reference's GeoCreateByStr (src/Geometry.c:37-88).
