@@ -12,6 +12,7 @@ for p in (ROOT, os.path.join(ROOT, "oracle"), os.path.join(ROOT, "lbm-benchmark-
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
     config.addinivalue_line("markers", "slow: takes more than a few seconds on CPU")
+    config.addinivalue_line("markers", "big: full-size workload (runs in the -m gpu pass; minutes of host CPU)")
 
 
 @pytest.fixture(scope="session")

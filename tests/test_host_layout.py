@@ -127,3 +127,36 @@ def test_pad_strings():
     assert L.lbmh_pad_cells(1000, 8, b"64+8") == 1001  # to the next multiple of 8 cells, plus one
     assert L.lbmh_pad_cells(1000, 8, b"64+64") == -1   # offset >= modulus is rejected
     assert L.lbmh_pad_cells(1000, 8, b"abc") == -1
+
+
+@pytest.mark.parametrize("pull", [0, 1])
+def test_packing_layout_matches_reference(reference, pull):
+    # a seeded periodic sphere packing (r in [6, 12], porosity 0.40): the host
+    # builder's numbering and adjacency equal the reference's Init bit for bit
+    lat, _ = lbmb200.spheres((64, 64, 64), 20251203, 0.40, 6.0, 12.0)
+    kernel = "list-pull-split-nt-1s-soa" if pull else "list-aa-pv-soa"
+    g1, a1, nf1, nc1 = lbmb200.list_build(lat, pull)
+    g2, a2, nf2, nc2 = reference.list_layout(kernel, lat.dims, lat.periodic, lat.mask)
+    assert (nf1, nc1) == (nf2, nc2) == (lat.n_fluid, nc2)
+    assert np.array_equal(g1, g2)
+    assert np.array_equal(a1, a2)
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("pull", [0, 1])
+def test_packing_256_layout_matches_reference_fixture(pull):
+    # the 256^3 packing of the throughput workload: the host builder's layout
+    # hashes equal those of the reference's Init (tests/golden/packing256.json,
+    # written by tests/golden/make_packing_golden.py)
+    import hashlib
+    import json
+    path = os.path.join(ROOT, "tests", "golden", "packing256.json")
+    with open(path) as f:
+        meta = json.load(f)
+    lat, _ = lbmb200.spheres((meta["edge"],) * 3, meta["seed"], 0.40, 6.0, 12.0)
+    assert hashlib.sha256(lat.mask.tobytes()).hexdigest() == meta["mask_sha256"]
+    lay = meta["layouts"]["pull" if pull else "push"]
+    g, a, nf, nc = lbmb200.list_build(lat, pull)
+    assert (nf, nc) == (lay["n_fluid"], lay["n_cells"])
+    assert hashlib.sha256(g.tobytes()).hexdigest() == lay["grid_sha256"]
+    assert hashlib.sha256(a.tobytes()).hexdigest() == lay["adj_sha256"]
