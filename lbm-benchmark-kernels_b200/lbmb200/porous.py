@@ -3,7 +3,10 @@ reference, which benchmarks fixed-length runs only).
 
 A solve drives the flow with a body force F along x until the mean velocity
 settles: it stops when the relative change of the mean x velocity over the
-last `check_every` steps drops below `tol`, or after `cap` steps. Mass and
+last `check_every` steps drops below `tol` (status "converged"), after `cap`
+steps ("not_converged"), or as soon as the FP64 sums are not finite
+("diverged": an unstable relaxation rate or a corrupt initial field; the
+domain then holds NaN or Inf and would never meet the tolerance). Mass and
 momentum are summed on the GPU in FP64 (lbm_b200_moments_device for the FP64
 kernel, the batch's per-domain sums for reduced storage).
 
@@ -13,6 +16,7 @@ and u_x = j_x + F/2 per node (the half-force correction the reference also
 applies to its velocity profile, src/Kernel.c:488-493), nu = (1/omega - 1/2)/3.
 """
 import ctypes
+import math
 import time
 
 import numpy as np
@@ -31,6 +35,20 @@ def mean_ux(jx_sum, n_fluid, xforce):
 def permeability(jx_sum, n_fluid, n_total, omega, xforce):
     q = (jx_sum + n_fluid * 0.5 * xforce) / n_total
     return viscosity(omega) * q / xforce
+
+
+CONVERGED, NOT_CONVERGED, DIVERGED = "converged", "not_converged", "diverged"
+
+
+def stop_status(u, prev, steps, tol, cap):
+    """The stopping rule after a check: None (keep going) or the status."""
+    if not math.isfinite(u):
+        return DIVERGED
+    if prev is not None and abs(u - prev) <= tol * abs(u):
+        return CONVERGED
+    if steps >= cap:
+        return NOT_CONVERGED
+    return None
 
 
 def request_domain(seed, edge, porosity, rmin=3.0, rmax=8.0):
@@ -64,34 +82,45 @@ class _Fp64Solver:
 from . import W as _W  # noqa: E402
 
 
-def solve_fp64(lattice, omega=1.0, lam=3.0 / 16.0, xforce=1e-5, check_every=100, tol=1e-6, cap=20000):
-    """Steady-state permeability with the FP64 kernel; returns dict."""
+def solve_fp64(lattice, omega=1.0, lam=3.0 / 16.0, xforce=1e-5, check_every=100, tol=1e-6, cap=20000,
+               initial_field=None):
+    """Steady-state permeability with the FP64 kernel; returns dict with the
+    status (k is None for a diverged solve). initial_field: PDFs to start
+    from instead of the equilibrium f_i = w_i."""
     s = _Fp64Solver(lattice, omega, lam, xforce)
     try:
+        if initial_field is not None:
+            s.inst.set_field(initial_field)
         prev, steps, t0 = None, 0, time.perf_counter()
         while True:
             s.step(check_every)
             steps += check_every
-            u = mean_ux(s.jx(), lattice.n_fluid, xforce)
-            if prev is not None and abs(u - prev) <= tol * abs(u) or steps >= cap:
+            jx = s.jx()
+            u = mean_ux(jx, lattice.n_fluid, xforce)
+            status = stop_status(u, prev, steps, tol, cap)
+            if status:
                 break
             prev = u
-        k = permeability(s.jx(), lattice.n_fluid, lattice.mask.size, omega, xforce)
-        return {"k": k, "steps": steps, "u": u, "seconds": time.perf_counter() - t0}
+        k = None if status == DIVERGED else permeability(jx, lattice.n_fluid, lattice.mask.size, omega, xforce)
+        return {"k": k, "steps": steps, "u": u, "status": status, "seconds": time.perf_counter() - t0}
     finally:
         s.close()
 
 
 def solve_batched(lattices, storage="fp32", omegas=None, lam=3.0 / 16.0, xforce=1e-5, check_every=100, tol=1e-6,
-                  cap=20000, budget_gb=150.0):
+                  cap=20000, budget_gb=150.0, initial_fields=None):
     """Steady-state permeabilities of several domains solved together in one
-    batch; returns one dict per domain (same stopping rule as solve_fp64)."""
+    batch; returns one dict per domain (same stopping rule as solve_fp64).
+    initial_fields: optional list of PDF fields (None = equilibrium)."""
     omegas = omegas or [1.0] * len(lattices)
     b = Batch(storage, budget_gb=budget_gb, max_domains=max(1, len(lattices)))
     try:
         slots = [b.add(l, omega=o, lam=lam, xforce=xforce) for l, o in zip(lattices, omegas)]
         if min(slots) < 0:
             raise RuntimeError("domains do not fit the batch")
+        for s, f in zip(slots, initial_fields or []):
+            if f is not None:
+                b.set_field(s, f)
         live = {s: i for i, s in enumerate(slots)}
         prev, steps, res = {}, 0, [None] * len(lattices)
         while live:
@@ -102,11 +131,12 @@ def solve_batched(lattices, storage="fp32", omegas=None, lam=3.0 / 16.0, xforce=
                 i = live[s]
                 lat = lattices[i]
                 u = mean_ux(mom[s][1], lat.n_fluid, xforce)
-                done = (s in prev and abs(u - prev[s]) <= tol * abs(u)) or steps >= cap
+                status = stop_status(u, prev.get(s), steps, tol, cap)
                 prev[s] = u
-                if done:
-                    res[i] = {"k": permeability(mom[s][1], lat.n_fluid, lat.mask.size, omegas[i], xforce),
-                              "steps": steps, "u": u}
+                if status:
+                    k = None if status == DIVERGED else permeability(mom[s][1], lat.n_fluid, lat.mask.size,
+                                                                     omegas[i], xforce)
+                    res[i] = {"k": k, "steps": steps, "u": u, "status": status}
                     b.remove(s)
                     del live[s]
         return res

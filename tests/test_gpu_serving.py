@@ -46,3 +46,51 @@ def test_server_completes_stream_under_tight_budget():
         lat = _lat(q.seed, q.edge, q.porosity)
         alone = porous.solve_batched([lat], omegas=[q.omega], tol=TOL)[0]
         assert alone["k"] == r["k"] and alone["steps"] == r["steps"]
+
+
+def _poisoned(field_of):
+    """initial_field hook: equilibrium everywhere, NaN in one PDF of the first
+    fluid cell of the requests in `field_of` (a host-side injection through
+    SetNode-equivalent field upload; no device fault is involved)."""
+    def init(req, lat):
+        if req.id not in field_of:
+            return None
+        f = np.array(np.broadcast_to(lbmb200.W, (lat.mask.size, 19)))
+        f[int(np.flatnonzero(lat.mask)[0]), 2] = np.nan
+        return f
+    return init
+
+
+def test_diverged_request_retires_at_its_first_check():
+    reqs = serving.make_requests(4, rate=0.0, seed=5, edge_range=(20, 32), omega_range=(0.8, 1.6))
+    summary, recs = serving.serve_batched(reqs, max_active=4, tol=TOL, closed_loop=True, prep_threads=2,
+                                          initial_field=_poisoned({1}))
+    by_id = {r["id"]: r for r in recs}
+    assert summary["solves"] == 4 and summary["status"].get("diverged") == 1
+    bad = by_id[1]
+    assert bad["status"] == "diverged" and bad["k"] is None and bad["steps"] == 100
+    # the others are untouched by their poisoned neighbour: bit for bit their solo results
+    for i in (0, 2, 3):
+        q = reqs[i]
+        alone = porous.solve_batched([_lat(q.seed, q.edge, q.porosity)], omegas=[q.omega], tol=TOL)[0]
+        assert by_id[i]["status"] == alone["status"] == "converged"
+        assert by_id[i]["k"] == alone["k"] and by_id[i]["steps"] == alone["steps"]
+
+
+def test_fp64_solver_reports_divergence():
+    lat = _lat(11, 24, 0.45)
+    f = np.array(np.broadcast_to(lbmb200.W, (lat.mask.size, 19)))
+    f[int(np.flatnonzero(lat.mask)[0]), 5] = np.inf
+    res = porous.solve_fp64(lat, tol=TOL, initial_field=f)
+    assert res["status"] == "diverged" and res["k"] is None and res["steps"] == 100
+    ok = porous.solve_fp64(lat, tol=TOL)
+    assert ok["status"] == "converged" and ok["k"] > 0
+
+
+def test_sequential_fp64_server_statuses():
+    reqs = serving.make_requests(3, rate=0.0, seed=9, edge_range=(20, 28), omega_range=(0.8, 1.6))
+    summary, recs = serving.serve_fp64_sequential(reqs, tol=TOL, closed_loop=True, prep_threads=2,
+                                                  initial_field=_poisoned({2}))
+    by_id = {r["id"]: r for r in recs}
+    assert summary["latency_samples"] == 3
+    assert by_id[2]["status"] == "diverged" and by_id[0]["status"] == by_id[1]["status"] == "converged"
