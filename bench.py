@@ -23,7 +23,9 @@ force along x. The headline kernel is the list AA kernel
 
 `--impl reference` times the reference's CPU kernel alone on the same
 workload and prints its own line. For N>1 every rank runs its own domain (seed
-+ rank): no data moves between ranks, scaling is weak.
++ rank): no data moves between ranks, scaling is weak. Beside that headline,
+N>1 also reports "slabs": the one 256^3 lattice split into x-slabs over the
+ranks with halo messages over NCCL (strong scaling), serial and overlapped.
 """
 import argparse
 import ctypes
@@ -63,8 +65,10 @@ def parse():
     p.add_argument("--no-extra", action="store_true", help="skip the secondary kernel lines")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--batched", type=int, default=512, help="domains of the batched form (0 = skip)")
-    p.add_argument("--serving", type=int, default=24, help="requests of the serving form (0 = skip)")
+    p.add_argument("--serving", type=int, default=100, help="requests of the serving form (0 = skip)")
     p.add_argument("--precision-steps", type=int, default=20000, help="steps of the precision study (0 = skip)")
+    p.add_argument("--no-slabs", action="store_true",
+                   help="N>1: skip the one-lattice x-slab split (strong scaling) beside the replicas")
     return p.parse_args()
 
 
@@ -216,9 +220,28 @@ class _StdoutToStderr:
         os.close(self.saved)
 
 
+def host_cpus():
+    """One logical CPU per physical core among the CPUs this process may run
+    on (the first sibling of each core, from the sysfs topology), and a
+    description of the host's processor."""
+    allowed = sorted(os.sched_getaffinity(0))
+    seen, phys = set(), []
+    for c in allowed:
+        try:
+            with open("/sys/devices/system/cpu/cpu%d/topology/thread_siblings_list" % c) as f:
+                key = f.read().strip()
+        except OSError:
+            key = str(c)
+        if key not in seen:
+            seen.add(key)
+            phys.append(c)
+    return phys, {"model": cpu_model(), "logical_cpus": len(allowed), "physical_cores": len(phys)}
+
+
 def cpu_reference(lat, iterations, threads=None, variant=None, kernel="list-aa-pv-soa"):
     """A reference kernel (benchmark build; list-aa-pv-soa by default) on this
-    host's cores."""
+    host's physical cores, one OpenMP thread pinned per core (the reference's
+    -t <cores> -pin <list>)."""
     with _StdoutToStderr():
         return _cpu_reference(lat, iterations, threads, variant, kernel)
 
@@ -232,13 +255,29 @@ def _cpu_reference(lat, iterations, threads=None, variant=None, kernel="list-aa-
     if not reference_available(variant):
         return None
     ref = Reference(variant)
-    threads = ref.set_threads(threads or os.cpu_count() or 1)
+    phys, desc = host_cpus()
+    cpus = phys[:threads] if threads else phys
+    threads = ref.set_threads(len(cpus))
+    pin_failed = ref.pin(cpus[:threads])
     ref.run(kernel, lat.dims, lat.periodic, lat.mask, omega=1.0, xforce=1e-5,
             iterations=iterations, init="zero", want_pdfs=False)
     dur = ref.last_duration
     it = iterations + (iterations % 2)  # the AA loop runs whole pairs
     return {"mflups": lat.n_fluid * it / dur / 1e6, "seconds": dur, "iterations": it, "threads": threads,
-            "variant": variant}
+            "variant": variant, "pinned": "%d threads pinned one per physical core (cpus %s)%s"
+            % (threads, _cpu_ranges(cpus[:threads]), "" if pin_failed == 0 else ", %d pinnings failed" % pin_failed),
+            "host": desc}
+
+
+def _cpu_ranges(cpus):
+    out, i = [], 0
+    while i < len(cpus):
+        j = i
+        while j + 1 < len(cpus) and cpus[j + 1] == cpus[j] + 1:
+            j += 1
+        out.append(str(cpus[i]) if i == j else "%d-%d" % (cpus[i], cpus[j]))
+        i = j + 1
+    return ",".join(out)
 
 
 def aa_line(lbmb200, fl, args, kargs, dist, peak):
@@ -265,18 +304,33 @@ def aa_line(lbmb200, fl, args, kargs, dist, peak):
             iters = int(max(2, min(200, 5.0 * probe["mflups"] * 1e6 / fl.n_fluid)))
             r = cpu_reference(fl, iters + iters % 2, kernel="aa-vec-soa")
             out["cpu_reference"] = {"mflups": round(r["mflups"], 1), "cores": r["threads"],
-                                    "sample": "%d steps, reference aa-vec-soa (%s build)" % (r["iterations"], r["variant"])}
+                                    "sample": "%d steps, reference aa-vec-soa (%s build), %s"
+                                              % (r["iterations"], r["variant"], r["pinned"])}
     return out
 
 
 def cpu_model():
+    """The processor's name with its family/model/stepping (a virtual machine
+    may report only a generic name) and, where sysfs has it, the socket count."""
+    info = {}
     try:
         for line in open("/proc/cpuinfo"):
-            if line.startswith("model name"):
-                return line.split(":", 1)[1].strip()
+            k, _, v = line.partition(":")
+            k = k.strip()
+            if k in ("model name", "cpu family", "model", "stepping") and k not in info:
+                info[k] = v.strip()
     except OSError:
-        pass
-    return "unknown"
+        return "unknown"
+    sockets = set()
+    for c in sorted(os.sched_getaffinity(0)):
+        try:
+            with open("/sys/devices/system/cpu/cpu%d/topology/physical_package_id" % c) as f:
+                sockets.add(f.read().strip())
+        except OSError:
+            pass
+    return "%s (family %s, model %s, stepping %s%s)" % (
+        info.get("model name", "unknown"), info.get("cpu family", "?"), info.get("model", "?"),
+        info.get("stepping", "?"), ", %d socket(s)" % len(sockets) if sockets else "")
 
 
 # ---------------------------------------------------------------------------
@@ -361,21 +415,28 @@ def section_batched(args, dist, peak):
 
 def section_serving(args, dist, peak):
     """Continuous batching (FP32) against the plain FP64 kernel one request at a
-    time, on the same seeded open-loop stream at 80 % of measured capacity."""
+    time, on the same seeded open-loop stream at 80 % of measured capacity.
+    Both servers prepare packings on 8 host threads from each request's
+    arrival on, so the ratio compares the GPU work, not host preparation."""
     from lbmb200 import serving
     n = args.serving
+    om = (0.8, 1.6)
     # capacity: the batched server with every request available at t = 0
-    cap_reqs = serving.make_requests(n, rate=0.0, seed=900 + dist.rank)
+    cap_reqs = serving.make_requests(n, rate=0.0, seed=900 + dist.rank, omega_range=om)
     cap_sum, _ = serving.serve_batched(cap_reqs, closed_loop=True, prep_threads=8)
     rate = 0.8 * cap_sum["solves_per_s"]
-    reqs = serving.make_requests(n, rate=rate, seed=901 + dist.rank)
+    reqs = serving.make_requests(n, rate=rate, seed=901 + dist.rank, omega_range=om)
     batched, recs = serving.serve_batched(reqs, prep_threads=8)
-    fp64, recs64 = serving.serve_fp64_sequential(reqs)
+    fp64, recs64 = serving.serve_fp64_sequential(reqs, prep_threads=8)
     by_id = {r["id"]: r for r in recs64}
-    kerr = max(abs(r["k"] - by_id[r["id"]]["k"]) / abs(by_id[r["id"]]["k"]) for r in recs)
+    both = [r for r in recs if r["k"] is not None and by_id[r["id"]]["k"] is not None]
+    kerr = max((abs(r["k"] - by_id[r["id"]]["k"]) / abs(by_id[r["id"]]["k"]) for r in both), default=None)
     return {"requests": n, "arrivals": "Poisson, %.3f/s (0.8 x measured capacity %.3f/s)"
                                       % (rate, cap_sum["solves_per_s"]),
-            "domain": "edge U{32..192}, porosity U[0.3,0.6], r U[3,8], F_x=1e-5, tol 1e-6 per 100 steps, cap 20000",
+            "domain": "edge U{32..192}, porosity U[0.3,0.6], r U[3,8], omega U[0.8,1.6], F_x=1e-5, "
+                      "tol 1e-6 per 100 steps, cap 20000",
+            "preparation": "both servers: packings built on 8 host threads from each request's arrival on",
+            "p99_note": "p99 over %d latency samples" % batched["latency_samples"],
             "batched_fp32": batched, "fp64_one_at_a_time": fp64,
             "solves_per_s_ratio": round(batched["solves_per_s"] / fp64["solves_per_s"], 3),
             "max_rel_permeability_diff_fp32_vs_fp64": kerr}
@@ -389,6 +450,124 @@ def section_precision(args, dist, peak):
     res = porous.precision_study(lat, steps=args.precision_steps, xforce=1e-5)
     res["steps"] = args.precision_steps
     return res
+
+
+# ---------------------------------------------------------------------------
+# one lattice over the ranks (x-slabs, strong scaling)
+
+class CudaSlabBackend:
+    """Slabs on this rank's GPU: the library's list-layout slab, an explicit
+    stream that is also torch's current stream, NCCL messages through
+    DistTransport, CUDA events for the timing."""
+
+    def __init__(self, dist):
+        import torch
+        self.torch = torch
+        torch.cuda.set_device(dist.local)
+        self.work = torch.cuda.Stream()
+        torch.cuda.set_stream(self.work)
+        self.stream = self.work.cuda_stream
+
+    def slab(self, lat, x0, x1, lo, hi, kargs):
+        import numpy as np
+
+        import lbmb200
+        from lbmb200 import slabs as sl
+        s = sl.Slab(lat, x0, x1, lo, hi, kernel_args=kargs, layout="list")
+        s.inst.set_field(np.broadcast_to(lbmb200.W, (s.local.mask.size, 19)))
+        return s
+
+    def transport(self, slab, rank, world, ring):
+        import torch.distributed
+        from lbmb200 import slabs as sl
+        return sl.DistTransport(slab, rank, world, ring, torch.distributed,
+                                lambda n: self.torch.empty(n, dtype=self.torch.float64, device="cuda"),
+                                stream=self.stream)
+
+    def mark(self):
+        e = self.torch.cuda.Event(enable_timing=True)
+        e.record(self.work)
+        return e
+
+    def sync(self):
+        self.torch.cuda.synchronize()
+
+    @staticmethod
+    def ms(a, b):
+        return a.elapsed_time(b)
+
+    def close(self, slab):
+        slab.close()
+
+
+class _TimedTransport:
+    """Marks the stream around each exchange operation of a transport (the
+    packs, the posting, the wait and the unpacks), so that the share of the
+    run spent on messages can be read off afterwards; nothing is skipped."""
+
+    def __init__(self, tr, backend):
+        self.tr, self.b, self.spans = tr, backend, []
+
+    def _timed(self, fn, phase):
+        m0 = self.b.mark()
+        fn(phase)
+        self.spans.append((m0, self.b.mark()))
+
+    def exchange(self, phase):
+        self._timed(self.tr.exchange, phase)
+
+    def start(self, phase):
+        self._timed(self.tr.start, phase)
+
+    def finish(self, phase):
+        self._timed(self.tr.finish, phase)
+
+
+def section_slabs(args, dist, backend=None, lat=None, pairs=20, warmup=3):
+    """The indirect-addressing workload's lattice (list layout, FP64) split
+    into x-slabs, one per rank, halo messages between neighbouring ranks:
+    serial (exchange after each half step) and overlapped (messages travel
+    while the inner tiles step). Every rank builds the same lattice (the
+    headline seed, not seed + rank) and takes its slab; times are the max
+    over ranks of the device-timed pairs."""
+    from lbmb200 import slabs as sl
+    import lbmb200
+    backend = backend or CudaSlabBackend(dist)
+    if lat is None:
+        lat, _ = sphere_lattice(lbmb200, args.edge, args.porosity, args.seed)
+    x0, x1 = sl.partition(lat.dims[0], dist.world)[dist.rank]
+    ring = sl.is_ring(lat.periodic)
+    lo, hi = sl.halo_flags(dist.rank, dist.world, ring)
+    slab = backend.slab(lat, x0, x1, lo, hi, ["-lambda", "3/16"])
+    try:
+        tr = _TimedTransport(backend.transport(slab, dist.rank, dist.world, ring), backend)
+        cd = lbmb200.case(omega=1.0, xforce=1e-5)
+        nodes = dist.sum(slab.local.n_fluid)
+        out = {"workload": "%d^3 sphere packing (seed %d), list layout, FP64, split in x over %d ranks"
+                           % (args.edge, args.seed, dist.world),
+               "scaling": "strong", "fluid_nodes": nodes, "pairs": pairs,
+               "slab_planes": [x0, x1], "layout": "list"}
+        for overlap in (False, True):
+            sl.step_pairs([slab], tr, cd, warmup, backend.stream, overlap=overlap)
+            backend.sync()
+            tr.spans = []
+            dist.barrier()
+            e0 = backend.mark()
+            sl.step_pairs([slab], tr, cd, pairs, backend.stream, overlap=overlap)
+            e1 = backend.mark()
+            backend.sync()
+            own = backend.ms(e0, e1)
+            exch = sum(backend.ms(a, b) for a, b in tr.spans)
+            ms = dist.max(own)
+            key = "overlapped" if overlap else "serial"
+            out[key] = {"ms": round(ms, 4), "mflups": round(nodes * 2 * pairs / (ms / 1e3) / 1e6, 1),
+                        "mflups_per_rank": round(nodes * 2 * pairs / (ms / 1e3) / 1e6 / dist.world, 1),
+                        "exchange_share": round(dist.max(exch / own if own > 0 else 0.0), 4)}
+        out["exchange_share_note"] = ("time of the stream between the marks around each exchange operation "
+                                      "(packs, posting, waiting, unpacks) over the pairs' time, max over ranks")
+        return out
+    finally:
+        backend.close(slab)
 
 
 # ---------------------------------------------------------------------------
@@ -423,8 +602,9 @@ def run_reference_arm(args, dist):
             "kernel": "reference list-aa-pv-soa (%s build; its Lambda is fixed at 1/12, which does not change "
                       "the work per step)" % r["variant"],
             "cpu_baseline": {"value": round(r["mflups"], 3), "unit": "MFLUP/s", "cores": r["threads"],
-                             "kind": "reference", "sample": "%d steps of the full domain" % r["iterations"],
-                             "cpu": cpu_model()},
+                             "kind": "reference", "sample": "%d steps of the full domain, %s"
+                                                            % (r["iterations"], r["pinned"]),
+                             "cpu": r["host"]},
             "e2e": {"value": round(r["mflups"], 3), "unit": "MFLUP/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -491,8 +671,11 @@ def run_ours(args, dist):
                      "even_step": {"bytes_per_flup": B_PER_FLUP["even"], "launch_ms": round(even_ms, 5),
                                    "achieved": round(B_PER_FLUP["even"] * lat.n_fluid / (even_ms / 1e3) / 1e9, 1)}},
         "e2e": {"value": round(nf_total * e2e_iters / e2e_s / 1e6, 3), "unit": "MFLUP/s",
-                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "step": "one Kernel() call of 500 time steps with PDF upload and download"},
+                "h2d_bytes_per_step": int(round(h2d / e2e_iters)), "d2h_bytes_per_step": int(round(d2h / e2e_iters)),
+                "h2d_bytes_per_call": int(h2d), "d2h_bytes_per_call": int(d2h), "steps_per_call": e2e_iters,
+                "call": "one Kernel() call of %d time steps: the PDF field uploaded from the pinned host mirror "
+                        "before the steps and downloaded after them (the bytes per step are the call's bytes "
+                        "over its steps)" % e2e_iters},
         "gpu_launches": t["launches"],
         "clocks": clk,
     }
@@ -554,7 +737,8 @@ def run_ours(args, dist):
 
     for name, fn, enabled in (("batched", section_batched, args.batched > 0),
                               ("serving", section_serving, args.serving > 0),
-                              ("precision", section_precision, args.precision_steps > 0 and dist.world == 1)):
+                              ("precision", section_precision, args.precision_steps > 0 and dist.world == 1),
+                              ("slabs", lambda a, d, p: section_slabs(a, d), dist.world > 1 and not args.no_slabs)):
         if not enabled:
             continue
         try:
@@ -571,7 +755,8 @@ def run_ours(args, dist):
             line["cpu_baseline"] = {"value": round(r["mflups"], 3), "unit": "MFLUP/s", "cores": r["threads"],
                                     "kind": "reference",
                                     "sample": "%d steps of the same domain, reference list-aa-pv-soa (%s build), %s"
-                                              % (r["iterations"], r["variant"], cpu_model())}
+                                              % (r["iterations"], r["variant"], r["pinned"]),
+                                    "cpu": r["host"]}
     if dist.rank == 0:
         print(json.dumps(line))
     return 0

@@ -30,6 +30,7 @@ torch.distributed -- NCCL on GPUs, gloo on CPU for the host-side tests).
 The slabs close into a ring (the first and last slab exchange too) when any
 axis is periodic (``is_ring``).
 """
+import contextlib
 import ctypes
 
 import numpy as np
@@ -228,7 +229,14 @@ class DistTransport:
     """One slab per rank: paired isend/irecv with the left and right
     neighbours through torch.distributed. Sends are posted right face first,
     receives left face first, so that two messages between the same pair of
-    ranks (two slabs on a periodic ring) match in order."""
+    ranks (two slabs on a periodic ring) match in order.
+
+    Stream order (NCCL): a posted send waits for torch's current stream, and
+    ``req.wait()`` makes only the current stream wait for the received
+    data. With an explicit `stream` (the slab's packs, unpacks and steps run
+    there), ``start`` and ``finish`` make that stream torch's current one for
+    their duration, so the sends follow the packs and the unpacks follow the
+    receives whatever stream the caller has current."""
 
     def __init__(self, slab, rank, world, ring, dist, make_buf, stream=None):
         self.slab, self.dist, self.stream = slab, dist, stream
@@ -242,10 +250,20 @@ class DistTransport:
         self.start(phase, sync)
         self.finish(phase)
 
+    def _on_stream(self):
+        if not self.stream:
+            return contextlib.nullcontext()
+        import torch
+        return torch.cuda.stream(torch.cuda.ExternalStream(self.stream))
+
     def start(self, phase, sync=None):
         """Packs this slab's messages and posts the sends and receives; they
         travel while the caller enqueues more work (with NCCL the library's
-        stream waits for the packs, then runs beside the caller's stream)."""
+        stream waits for the packs, then runs beside the slab's stream)."""
+        with self._on_stream():
+            self._start(phase, sync)
+
+    def _start(self, phase, sync):
         d = self.dist
         faces = [s for s in (1, 0) if (self.right if s else self.left) is not None]
         out = {s: self.send[s][:message(self.slab, s, phase, True)] for s in faces}
@@ -264,8 +282,12 @@ class DistTransport:
         self._reqs = d.batch_isend_irecv(ops) if ops else []
 
     def finish(self, phase):
-        """Waits for the posted messages (on NCCL: the caller's stream waits)
+        """Waits for the posted messages (on NCCL: the slab's stream waits)
         and unpacks the received ones."""
+        with self._on_stream():
+            self._finish(phase)
+
+    def _finish(self, phase):
         for req in self._reqs:
             req.wait()
         self._reqs = []

@@ -82,6 +82,34 @@ class EmuSlab:
         self.f[self.idx(side, phase, False)] = buf.numpy()
 
 
+class SteppedEmuSlab:
+    """An EmuSlab behind the library slab's step interface (step, odd_part,
+    even_part with lbmb200.slabs.Slab's signatures; cd and stream unused), so
+    that lbmb200.slabs.step_pairs drives the oracle-stepped slab exactly as
+    it drives a GPU slab."""
+
+    def __init__(self, emu, oracle):
+        self.emu, self.oracle = emu, oracle
+
+    def step(self, cd, half, stream=None):
+        self.emu.half(self.oracle, half)
+
+    def odd_part(self, cd, part, stream=None):
+        self.emu.odd_part(self.oracle, part)
+
+    def even_part(self, cd, part, stream=None):
+        self.emu.even_part(self.oracle, part)
+
+    def message(self, side, phase, send):
+        return self.emu.message(side, phase, send)
+
+    def pack(self, side, phase, buf, stream=None):
+        self.emu.pack(side, phase, buf, stream)
+
+    def unpack(self, side, phase, buf, stream=None):
+        self.emu.unpack(side, phase, buf, stream)
+
+
 def exchange(slabs, faces, phase):
     """The two-phase exchange between in-process slabs: faces are (r, q)
     pairs, q the right-hand neighbour of r."""

@@ -83,7 +83,7 @@ LIST_SCRIPT = textwrap.dedent("""
     from lbmb200.ranks import Ranks
     from lbmb200 import slabs as sl
     from oracle import Oracle
-    from slab_emu import EmuSlab, init_field
+    from slab_emu import EmuSlab, SteppedEmuSlab, init_field
 
     r = Ranks(backend="gloo", timeout_s=60)
     geo, dims, per, pairs = sys.argv[1], tuple(int(v) for v in sys.argv[2].split("x")), \\
@@ -95,27 +95,9 @@ LIST_SCRIPT = textwrap.dedent("""
     slab = EmuSlab(lat, x0, x1, lo, hi, ("-pad", "no"))
     slab.set_field(init_field(lat, 5))
     tr = sl.DistTransport(slab, r.rank, r.world, ring, dist, lambda n: torch.zeros(n, dtype=torch.float64))
-    orc = Oracle()
     overlap = len(sys.argv) > 5 and sys.argv[5] == "1"
-    if overlap:
-        slab.half(orc, 0)
-        for k in range(pairs):
-            tr.start(0)
-            slab.odd_part(orc, 0)
-            tr.finish(0)
-            slab.odd_part(orc, 1)
-            tr.start(1)
-            if k + 1 < pairs:
-                slab.even_part(orc, 0)
-            tr.finish(1)
-            if k + 1 < pairs:
-                slab.even_part(orc, 1)
-    else:
-        for _ in range(pairs):
-            slab.half(orc, 0)
-            tr.exchange(0)
-            slab.half(orc, 1)
-            tr.exchange(1)
+    # the library's own step sequence (serial or overlapped) drives the slab
+    sl.step_pairs([SteppedEmuSlab(slab, Oracle())], tr, None, pairs, None, overlap=overlap)
     out = np.zeros((lat.mask.size, 19))
     slab.get_field(out)
     np.save(os.path.join(%(out)r, "part%%d.npy" %% r.rank), out[slab.gcells])
@@ -131,10 +113,11 @@ LIST_SCRIPT = textwrap.dedent("""
                                                          (3, "channel", "24x16x16", "110", 1)])
 def test_list_slabs_over_gloo_match_undivided_run(tmp_path, oracle, world, geo, dims, per, overlap):
     """List-AA slabs as gloo ranks: the layout from the library, the steps
-    from the oracle, the halo messages through DistTransport (with `overlap`,
-    the phase-0 messages are posted, the inner tiles step, then the messages
-    are awaited and the other tiles step); the gathered field equals the
-    undivided oracle run bit for bit."""
+    from the oracle, the step sequence from lbmb200.slabs.step_pairs and the
+    halo messages through DistTransport's asynchronous start/finish (with
+    `overlap`, the phase-0 messages are posted, the inner tiles step, then
+    the messages are awaited and the other tiles step); the gathered field
+    equals the undivided oracle run bit for bit."""
     sys.path[:0] = [os.path.join(ROOT, "tests")]
     import numpy as np
     import lbmb200
