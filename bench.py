@@ -220,10 +220,20 @@ class _StdoutToStderr:
         os.close(self.saved)
 
 
+_HOST_CPUS = None
+
+
 def host_cpus():
     """One logical CPU per physical core among the CPUs this process may run
     on (the first sibling of each core, from the sysfs topology), and a
-    description of the host's processor."""
+    description of the host's processor. Taken once, before any pinning."""
+    global _HOST_CPUS
+    if _HOST_CPUS is None:
+        _HOST_CPUS = _host_cpus()
+    return _HOST_CPUS
+
+
+def _host_cpus():
     allowed = sorted(os.sched_getaffinity(0))
     seen, phys = set(), []
     for c in allowed:
@@ -258,9 +268,16 @@ def _cpu_reference(lat, iterations, threads=None, variant=None, kernel="list-aa-
     phys, desc = host_cpus()
     cpus = phys[:threads] if threads else phys
     threads = ref.set_threads(len(cpus))
-    pin_failed = ref.pin(cpus[:threads])
-    ref.run(kernel, lat.dims, lat.periodic, lat.mask, omega=1.0, xforce=1e-5,
-            iterations=iterations, init="zero", want_pdfs=False)
+    # the OpenMP master is this thread: pinning it for the reference's run
+    # must not confine the rest of the process (host threads of the serving
+    # and batched sections start from its affinity), so it is restored after
+    saved = os.sched_getaffinity(0)
+    try:
+        pin_failed = ref.pin(cpus[:threads])
+        ref.run(kernel, lat.dims, lat.periodic, lat.mask, omega=1.0, xforce=1e-5,
+                iterations=iterations, init="zero", want_pdfs=False)
+    finally:
+        os.sched_setaffinity(0, saved)
     dur = ref.last_duration
     it = iterations + (iterations % 2)  # the AA loop runs whole pairs
     return {"mflups": lat.n_fluid * it / dur / 1e6, "seconds": dur, "iterations": it, "threads": threads,

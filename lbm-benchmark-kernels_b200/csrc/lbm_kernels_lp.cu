@@ -110,8 +110,14 @@ __global__ void __launch_bounds__(256, 2) k_list_even_staged(const ListArgsLp a,
   }
 }
 
+// Resident blocks per SM the odd step is compiled for (6: the shared-memory
+// limit of its staged run record; the register cap follows from it).
+#ifndef LBM_LP_ODD_BLOCKS
+#define LBM_LP_ODD_BLOCKS 6
+#endif
+
 template <class St>
-__global__ void __launch_bounds__(kListTile, 6) k_list_odd_lp(const ListArgsLp a, const TrtW w) {
+__global__ void __launch_bounds__(kListTile, LBM_LP_ODD_BLOCKS) k_list_odd_lp(const ListArgsLp a, const TrtW w) {
   __shared__ alignas(128) uint32_t srun[kRunTileWords];
   __shared__ alignas(8) uint64_t bar;
   __shared__ int ok;

@@ -26,6 +26,12 @@
 #pragma once
 #include <cuda_fp16.h>
 
+// Whether the odd step reads a run's adjacency row from shared memory in
+// 8-byte pairs (1) or as 4-byte words (0).
+#ifndef LBM_LP_ROW_PAIRS
+#define LBM_LP_ROW_PAIRS 1
+#endif
+
 #include "lbm_d3q19.cuh"
 
 namespace lbm {
@@ -152,12 +158,17 @@ __device__ __forceinline__ void lp_odd_node(typename St::T* f, uint32_t S, uint3
   const uint32_t head = n - off;
   const uint2* const e2 = reinterpret_cast<const uint2*>(e);
   uint32_t l[QM];
+#if LBM_LP_ROW_PAIRS
 #pragma unroll
   for (int k = 0; k < QM / 2; ++k) {
     const uint2 v = e2[k];
     l[2 * k] = v.x;
     l[2 * k + 1] = v.y;
   }
+#else
+#pragma unroll
+  for (int k = 0; k < QM; ++k) l[k] = e[k];
+#endif
   float x[Q], o[Q];
   x[DC] = St::in(fo[DC * S + head], DC);
 #pragma unroll
@@ -171,7 +182,12 @@ __device__ __forceinline__ void lp_odd_node(typename St::T* f, uint32_t S, uint3
 #pragma unroll
   for (int k = 0; k < QM / 2; ++k) {
     // re-read from shared memory: keeps no links live across the collision
+#if LBM_LP_ROW_PAIRS
     const unsigned long long pr = reinterpret_cast<const volatile unsigned long long*>(e2)[k];
+#else
+    const unsigned long long pr = reinterpret_cast<const volatile uint32_t*>(e)[2 * k] |
+                                  (static_cast<unsigned long long>(reinterpret_cast<const volatile uint32_t*>(e)[2 * k + 1]) << 32);
+#endif
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int d = 2 * k + h;
