@@ -515,6 +515,8 @@ class CudaSlabBackend:
 
     def close(self, slab):
         slab.close()
+        self.torch.cuda.synchronize()
+        self.torch.cuda.set_stream(self.torch.cuda.default_stream())
 
 
 class _TimedTransport:

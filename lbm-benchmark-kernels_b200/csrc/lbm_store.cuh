@@ -26,12 +26,6 @@
 #pragma once
 #include <cuda_fp16.h>
 
-// Whether the odd step reads a run's adjacency row from shared memory in
-// 8-byte pairs (1) or as 4-byte words (0).
-#ifndef LBM_LP_ROW_PAIRS
-#define LBM_LP_ROW_PAIRS 1
-#endif
-
 #include "lbm_d3q19.cuh"
 
 namespace lbm {
@@ -141,34 +135,23 @@ __device__ __forceinline__ void lp_even_node(typename St::T* f, long long S, int
 }
 
 // Odd step of node n, whose links come run-compressed: link d = e[d] + off
-// (e: the run's adjacency row in shared memory, 8-byte aligned: rows start
-// at 48 + 72 k bytes of the record). The node reads f_d from link inv(d)
+// (e: the run's adjacency row in shared memory). The node reads f_d from link inv(d)
 // plus its body-force increment and writes f_d to link d. A link is either
 // the neighbour's slot in plane d or -- bounce back -- the node's own slot
 // in plane inv(d); the PDF then gets the increment of inv(d), which differs
 // from d's only for c_x != 0, so only those ten directions test it, by the
 // link's plane (one compare against a constant per direction). Addresses
-// are formed from f + off, so a link costs one multiply-add on top of its
-// shared-memory read; the row is read as 8-byte pairs.
+// are formed from f + off, so a link costs one index on top of its
+// shared-memory read.
 template <class St>
 __device__ __forceinline__ void lp_odd_node(typename St::T* f, uint32_t S, uint32_t n, const uint32_t* e,
                                             uint32_t off, const TrtDev<St>& t) {
   using T = typename St::T;
   T* const fo = f + off;  // every address below is fo + 32-bit index (the node itself: DC * S + head)
   const uint32_t head = n - off;
-  const uint2* const e2 = reinterpret_cast<const uint2*>(e);
   uint32_t l[QM];
-#if LBM_LP_ROW_PAIRS
-#pragma unroll
-  for (int k = 0; k < QM / 2; ++k) {
-    const uint2 v = e2[k];
-    l[2 * k] = v.x;
-    l[2 * k + 1] = v.y;
-  }
-#else
 #pragma unroll
   for (int k = 0; k < QM; ++k) l[k] = e[k];
-#endif
   float x[Q], o[Q];
   x[DC] = St::in(fo[DC * S + head], DC);
 #pragma unroll
@@ -180,26 +163,16 @@ __device__ __forceinline__ void lp_odd_node(typename St::T* f, uint32_t S, uint3
   T* const fs = launder(fo);
   fs[DC * S + head] = St::out(o[DC], DC);
 #pragma unroll
-  for (int k = 0; k < QM / 2; ++k) {
+  for (int d = 0; d < QM; ++d) {
     // re-read from shared memory: keeps no links live across the collision
-#if LBM_LP_ROW_PAIRS
-    const unsigned long long pr = reinterpret_cast<const volatile unsigned long long*>(e2)[k];
-#else
-    const unsigned long long pr = reinterpret_cast<const volatile uint32_t*>(e)[2 * k] |
-                                  (static_cast<unsigned long long>(reinterpret_cast<const volatile uint32_t*>(e)[2 * k + 1]) << 32);
-#endif
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int d = 2 * k + h;
-      const uint32_t ed = static_cast<uint32_t>(h ? pr >> 32 : pr);
-      float v = o[d];
-      if (cx(d) != 0) {
-        // plane inv(d) lies below plane d when inv(d) < d, above it otherwise
-        const bool bounce = inv(d) < d ? ed < static_cast<uint32_t>(d) * S : ed >= static_cast<uint32_t>(d + 1) * S;
-        v += bounce ? t.force(inv(d)) : t.force(d);
-      }
-      fs[ed] = St::out(v, d);  // the scale is equal for d and inv(d)
+    const uint32_t ed = reinterpret_cast<const volatile uint32_t*>(e)[d];
+    float v = o[d];
+    if (cx(d) != 0) {
+      // plane inv(d) lies below plane d when inv(d) < d, above it otherwise
+      const bool bounce = inv(d) < d ? ed < static_cast<uint32_t>(d) * S : ed >= static_cast<uint32_t>(d + 1) * S;
+      v += bounce ? t.force(inv(d)) : t.force(d);
     }
+    fs[ed] = St::out(v, d);  // the scale is equal for d and inv(d)
   }
 }
 
