@@ -25,7 +25,9 @@ force along x. The headline kernel is the list AA kernel
 workload and prints its own line. For N>1 every rank runs its own domain (seed
 + rank): no data moves between ranks, scaling is weak. Beside that headline,
 N>1 also reports "slabs": the one 256^3 lattice split into x-slabs over the
-ranks with halo messages over NCCL (strong scaling), serial and overlapped.
+ranks with halo messages over NCCL (strong scaling), serial and overlapped;
+the single-GPU sections (secondary kernel lines, batched, serving,
+precision, CPU baseline) run at N=1 only.
 """
 import argparse
 import ctypes
@@ -699,7 +701,10 @@ def run_ours(args, dist):
         "clocks": clk,
     }
 
-    if not args.no_extra:
+    # with several ranks the line carries the replica headline and the slab
+    # split; the secondary kernel lines, batched and serving sections are
+    # single-GPU measurements (every rank would repeat them on its own GPU)
+    if not args.no_extra and dist.world == 1:
         extra = {}
         # pull kernel on the same domain
         tp = time_kernel(lbmb200, "cuda-list-pull-split-nt-1s-soa", lat, min(args.steps, 200), 3, kargs, dist, "pull")
@@ -754,8 +759,8 @@ def run_ours(args, dist):
                 "odd_ms": round(statistics.mean(tl["per_launch_ms"][1::2]), 5)}
         line["kernels"] = extra
 
-    for name, fn, enabled in (("batched", section_batched, args.batched > 0),
-                              ("serving", section_serving, args.serving > 0),
+    for name, fn, enabled in (("batched", section_batched, args.batched > 0 and dist.world == 1),
+                              ("serving", section_serving, args.serving > 0 and dist.world == 1),
                               ("precision", section_precision, args.precision_steps > 0 and dist.world == 1),
                               ("slabs", lambda a, d, p: section_slabs(a, d), dist.world > 1 and not args.no_slabs)):
         if not enabled:
