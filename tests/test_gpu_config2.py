@@ -94,6 +94,24 @@ def test_packing_64_against_reference(reference):
         reference.set_threads(min(4, os.cpu_count() or 1))
 
 
+@pytest.mark.parametrize("kname,rkernel", [("cuda-list-push-soa", "list-push-soa"),
+                                           ("cuda-list-pull-soa", "list-pull-soa")])
+def test_packing_64_two_grid_list_rows_equal_reference(reference, kname, rkernel):
+    # the two-grid list rows (src/BenchKernelD3Q19List.c) on the packing, 500
+    # forced steps: bit for bit against the reference's scalar kernels
+    lat = _packing(64, PACKING_SEED)
+    init = random_pdfs(lat.mask.size, 66)
+    g, _ = _gpu_run(kname, lat, init, "1/12")
+    reference.set_threads(os.cpu_count() or 1)
+    try:
+        r = reference.run(rkernel, lat.dims, lat.periodic, lat.mask, omega=1.0, xforce=XFORCE, iterations=STEPS,
+                          init="pdfs", init_pdfs=init)
+    finally:
+        reference.set_threads(min(4, os.cpu_count() or 1))
+    m = lat.mask != 0
+    assert np.array_equal(g[m], r[m])
+
+
 @pytest.mark.parametrize("kname,okernel", [("cuda-list-aa-pv-soa", "list-aa"),
                                            ("cuda-list-pull-split-nt-1s-soa", "list-pull")])
 def test_packing_64_lambda_3_16_equals_oracle(oracle, kname, okernel):
