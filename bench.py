@@ -435,18 +435,22 @@ def section_batched(args, dist, peak):
 def section_serving(args, dist, peak):
     """Continuous batching (FP32) against the plain FP64 kernel one request at a
     time, on the same seeded open-loop stream at 80 % of measured capacity.
-    Both servers prepare packings on 8 host threads from each request's
-    arrival on, so the ratio compares the GPU work, not host preparation."""
+    Both servers prepare packings on the same number of host threads (one per
+    physical core but the serving loop's) from each request's arrival on, so
+    the ratio compares the GPU work, not host preparation."""
     from lbmb200 import serving
     n = args.serving
     om = (0.8, 1.6)
+    # host preparation (sphere packings, in C) on one thread per physical core
+    # but the one the serving loop itself runs on, alike for both servers
+    prep = max(1, len(host_cpus()[0]) - 1)
     # capacity: the batched server with every request available at t = 0
     cap_reqs = serving.make_requests(n, rate=0.0, seed=900 + dist.rank, omega_range=om)
-    cap_sum, _ = serving.serve_batched(cap_reqs, closed_loop=True, prep_threads=8)
+    cap_sum, _ = serving.serve_batched(cap_reqs, closed_loop=True, prep_threads=prep)
     rate = 0.8 * cap_sum["solves_per_s"]
     reqs = serving.make_requests(n, rate=rate, seed=901 + dist.rank, omega_range=om)
-    batched, recs = serving.serve_batched(reqs, prep_threads=8)
-    fp64, recs64 = serving.serve_fp64_sequential(reqs, prep_threads=8)
+    batched, recs = serving.serve_batched(reqs, prep_threads=prep)
+    fp64, recs64 = serving.serve_fp64_sequential(reqs, prep_threads=prep)
     by_id = {r["id"]: r for r in recs64}
     both = [r for r in recs if r["k"] is not None and by_id[r["id"]]["k"] is not None]
     kerr = max((abs(r["k"] - by_id[r["id"]]["k"]) / abs(by_id[r["id"]]["k"]) for r in both), default=None)
@@ -454,7 +458,8 @@ def section_serving(args, dist, peak):
                                       % (rate, cap_sum["solves_per_s"]),
             "domain": "edge U{32..192}, porosity U[0.3,0.6], r U[3,8], omega U[0.8,1.6], F_x=1e-5, "
                       "tol 1e-6 per 100 steps, cap 20000",
-            "preparation": "both servers: packings built on 8 host threads from each request's arrival on",
+            "preparation": "both servers: packings built on %d host threads (one per physical core but the "
+                           "serving loop's) from each request's arrival on" % prep,
             "p99_note": "p99 over %d latency samples" % batched["latency_samples"],
             "batched_fp32": batched, "fp64_one_at_a_time": fp64,
             "solves_per_s_ratio": round(batched["solves_per_s"] / fp64["solves_per_s"], 3),

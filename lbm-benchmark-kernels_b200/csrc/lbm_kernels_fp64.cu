@@ -65,11 +65,12 @@ __device__ __forceinline__ bool aa_open(const AaArgs& a, int x, int y, int z, in
   return (ox || oy || oz) && !crossesPeriodic;
 }
 
-// One block per 128 z-cells of a row (longer contiguous segments per plane
-// than 32 x 4 blocks), capped at 8 resident blocks per SM (64 registers):
-// 0.827 ms against 0.850 ms for 32 x 4 blocks at 256^3 on B200.
-__global__ void __launch_bounds__(128, 8) k_aa_even_fp64(const AaArgs a, const Trt<double> t) {
-  const int z = blockIdx.x * 128 + threadIdx.x;
+// One block per 256 z-cells of a row (longer contiguous segments per plane),
+// 4 resident blocks per SM (64 registers): 0.816 ms against 0.824 ms for
+// 128-cell blocks and 0.850 ms for 32 x 4 blocks at 256^3 on B200.
+constexpr int kAaEvenBlock = 256;
+__global__ void __launch_bounds__(kAaEvenBlock, 1024 / kAaEvenBlock) k_aa_even_fp64(const AaArgs a, const Trt<double> t) {
+  const int z = blockIdx.x * kAaEvenBlock + threadIdx.x;
   const int y = blockIdx.y;
   const int x = blockIdx.z + a.xBase;
   if (z >= a.nZ || y >= a.nY) return;
@@ -96,7 +97,7 @@ __global__ void __launch_bounds__(128, 8) k_aa_even_fp64(const AaArgs a, const T
 // is the neighbour's slot), the others are "general" (each address is a
 // select between the neighbour's slot and the node's own slot). The launch
 // runs a list of work items in x-plane order: for each plane, the blocks
-// (32 z-cells x 4 y-rows) that hold at least one direct cell -- these skip
+// (128 z-cells of one row) that hold at least one direct cell -- these skip
 // the general cells in them -- then chunks of 128 of the plane's general
 // cells, one thread per cell. So the select-free path covers every direct
 // cell, also those next to a wall (in a 256^3 channel a split by whole blocks
@@ -114,13 +115,18 @@ __global__ void __launch_bounds__(128, 8) k_aa_even_fp64(const AaArgs a, const T
 // reads and writes only its own links' slots), so the work items and the
 // two launches may run in any order.
 
+// Interior blocks of the odd step: kAaBZ z-cells x kAaBY rows of one x plane
+// (128 threads). A 128-cell row segment per plane: interior 0.811 ms against
+// 0.818 ms for 64 x 2 and 0.830 ms for 32 x 4 blocks (256^3 fluid box, B200).
+constexpr int kAaBZ = 128, kAaBY = 1;
+
 // Interior block `id` of the list: (bz, by, bx) with bz fastest.
 __device__ __forceinline__ void aa_interior_block(const AaArgs& a, int id, int& z, int& y, int& x) {
   const int nz = a.perZ ? a.nZ : a.nZ - 2;
-  const int gz = (nz + 31) / 32, gy = (a.nY - 2 + 3) / 4;
+  const int gz = (nz + kAaBZ - 1) / kAaBZ, gy = (a.nY - 2 + kAaBY - 1) / kAaBY;
   const int bz = id % gz, rest = id / gz;
-  z = (a.perZ ? 0 : 1) + bz * 32 + threadIdx.x;
-  y = 1 + (rest % gy) * 4 + threadIdx.y;
+  z = (a.perZ ? 0 : 1) + bz * kAaBZ + threadIdx.x;
+  y = 1 + (rest % gy) * kAaBY + threadIdx.y;
   x = 1 + rest / gy;
 }
 
@@ -175,7 +181,7 @@ __global__ void __launch_bounds__(128, 7)
                            const int* cells) {
   const int item = __ldg(items + blockIdx.x);
   if (item < 0) {
-    const int c = __ldg(cells + (size_t)(~item) * 128 + threadIdx.y * 32 + threadIdx.x);
+    const int c = __ldg(cells + (size_t)(~item) * 128 + threadIdx.y * kAaBZ + threadIdx.x);
     if (c >= 0) aa_odd_general_cell(a, t, c);
     return;
   }
@@ -441,7 +447,7 @@ bool aa_has_interior(const AaArgs& a) { return a.nX > 2 && a.nY > 2 && (a.perZ |
 long long aa_interior_block_count(const AaArgs& a) {
   if (!aa_has_interior(a)) return 0;
   const long long nz = a.perZ ? a.nZ : a.nZ - 2;
-  return (nz + 31) / 32 * ((a.nY - 2 + 3) / 4) * (long long)(a.nX - 2);
+  return (nz + kAaBZ - 1) / kAaBZ * ((a.nY - 2 + kAaBY - 1) / kAaBY) * (long long)(a.nX - 2);
 }
 
 void aa_interior_items(const AaArgs& a, const uint32_t* link, std::vector<int>& items, std::vector<int>& cells) {
@@ -450,7 +456,7 @@ void aa_interior_items(const AaArgs& a, const uint32_t* link, std::vector<int>& 
   const long long n = aa_interior_block_count(a);
   if (n == 0) return;
   const int zLo = a.perZ ? 0 : 1, zHi = a.perZ ? a.nZ - 1 : a.nZ - 2;
-  const int gz = (zHi - zLo + 1 + 31) / 32, gy = (a.nY - 2 + 3) / 4;
+  const int gz = (zHi - zLo + 1 + kAaBZ - 1) / kAaBZ, gy = (a.nY - 2 + kAaBY - 1) / kAaBY;
   const long long perPlane = (long long)gz * gy;
   auto word = [&](int x, int y, int z) { return link[(long long)(x + 1) * a.xs + (long long)(y + 1) * a.pitch + z + kZOff]; };
   for (int x = 1; x <= a.nX - 2; ++x) {
@@ -458,11 +464,11 @@ void aa_interior_items(const AaArgs& a, const uint32_t* link, std::vector<int>& 
     for (long long k = 0; k < perPlane; ++k) {
       const int bz = (int)(k % gz), by = (int)(k / gz);
       bool direct = false;
-      for (int ty = 0; ty < 4 && !direct; ++ty) {
-        const int y = 1 + by * 4 + ty;
+      for (int ty = 0; ty < kAaBY && !direct; ++ty) {
+        const int y = 1 + by * kAaBY + ty;
         if (y > a.nY - 2) break;
-        for (int tz = 0; tz < 32; ++tz) {
-          const int z = zLo + bz * 32 + tz;
+        for (int tz = 0; tz < kAaBZ; ++tz) {
+          const int z = zLo + bz * kAaBZ + tz;
           if (z > zHi) break;
           if ((word(x, y, z) & (kFluidBit | kLinkBits)) == kFluidBit) { direct = true; break; }
         }
@@ -484,19 +490,19 @@ void aa_interior_items(const AaArgs& a, const uint32_t* link, std::vector<int>& 
 void aa_even_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
   AaArgs b = a;
   b.xBase = 0;
-  k_aa_even_fp64<<<dim3((a.nZ + 127) / 128, a.nY, a.nX), 128, 0, s>>>(b, t);
+  k_aa_even_fp64<<<dim3((a.nZ + kAaEvenBlock - 1) / kAaEvenBlock, a.nY, a.nX), kAaEvenBlock, 0, s>>>(b, t);
 }
 
 void aa_even_fp64_planes(const AaArgs& a, const Trt<double>& t, int x0, int x1, cudaStream_t s) {
   if (x1 <= x0) return;
   AaArgs b = a;
   b.xBase = x0;
-  k_aa_even_fp64<<<dim3((a.nZ + 127) / 128, a.nY, x1 - x0), 128, 0, s>>>(b, t);
+  k_aa_even_fp64<<<dim3((a.nZ + kAaEvenBlock - 1) / kAaEvenBlock, a.nY, x1 - x0), kAaEvenBlock, 0, s>>>(b, t);
 }
 
 void aa_odd_interior_fp64(const AaArgs& a, const Trt<double>& t, const int* items, int nItems, const int* cells,
                           cudaStream_t s) {
-  if (nItems > 0) k_aa_odd_interior_fp64<<<nItems, dim3(32, 4), 0, s>>>(a, t, items, cells);
+  if (nItems > 0) k_aa_odd_interior_fp64<<<nItems, dim3(kAaBZ, kAaBY), 0, s>>>(a, t, items, cells);
 }
 
 void aa_odd_face_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
