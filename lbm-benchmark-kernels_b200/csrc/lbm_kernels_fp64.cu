@@ -346,13 +346,19 @@ void aa_halo_unpack(const AaArgs& a, int side, int phase, const double* buf, cud
 // stores; the result in every slot some fluid node views is the reference's
 // bit for bit (tests against the oracle and the reference).
 
+// Blocks of the two-grid steps: kFaBZ z-cells x kFaBY rows of one x plane.
+// 32 x 4: push 0.860 / pull 0.897 ms at 256^3 (fluid box) against 0.867 /
+// 0.925 for 64 x 2 and 0.887 / 0.986 for 128 x 1 (unlike the AA steps, whose
+// longer row segments won).
+constexpr int kFaBZ = 32, kFaBY = 4;
+
 // Push: node x's own PDFs in from grid f; PDF d out to (x + c_d, d) of grid g
 // (across a periodic face: the wrapped cell). A wall sends it back to the
 // node's own slot inv(d); an open face leaves that slot untouched by the step,
 // so only the force increment is added to what the grid held.
 __global__ void __launch_bounds__(128) k_fa_push_fp64(const AaArgs a, const Trt<double> t) {
-  const int z = blockIdx.x * 32 + threadIdx.x;
-  const int y = blockIdx.y * 4 + threadIdx.y;
+  const int z = blockIdx.x * kFaBZ + threadIdx.x;
+  const int y = blockIdx.y * kFaBY + threadIdx.y;
   const int x = blockIdx.z;
   if (z >= a.nZ || y >= a.nY) return;
   const int c = aa_cell(a, x, y, z);
@@ -393,8 +399,8 @@ __global__ void __launch_bounds__(128) k_fa_push_fp64(const AaArgs a, const Trt<
 // image q = wrap(x + c_e) gets it at (q - c_e, e), and an open slot only gets
 // the force increment.
 __global__ void __launch_bounds__(128) k_fa_pull_fp64(const AaArgs a, const Trt<double> t) {
-  const int z = blockIdx.x * 32 + threadIdx.x;
-  const int y = blockIdx.y * 4 + threadIdx.y;
+  const int z = blockIdx.x * kFaBZ + threadIdx.x;
+  const int y = blockIdx.y * kFaBY + threadIdx.y;
   const int x = blockIdx.z;
   if (z >= a.nZ || y >= a.nY) return;
   const int c = aa_cell(a, x, y, z);
@@ -430,10 +436,10 @@ __global__ void __launch_bounds__(128) k_fa_pull_fp64(const AaArgs a, const Trt<
 }
 
 void fa_push_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
-  k_fa_push_fp64<<<dim3((a.nZ + 31) / 32, (a.nY + 3) / 4, a.nX), dim3(32, 4), 0, s>>>(a, t);
+  k_fa_push_fp64<<<dim3((a.nZ + kFaBZ - 1) / kFaBZ, (a.nY + kFaBY - 1) / kFaBY, a.nX), dim3(kFaBZ, kFaBY), 0, s>>>(a, t);
 }
 void fa_pull_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
-  k_fa_pull_fp64<<<dim3((a.nZ + 31) / 32, (a.nY + 3) / 4, a.nX), dim3(32, 4), 0, s>>>(a, t);
+  k_fa_pull_fp64<<<dim3((a.nZ + kFaBZ - 1) / kFaBZ, (a.nY + kFaBY - 1) / kFaBY, a.nX), dim3(kFaBZ, kFaBY), 0, s>>>(a, t);
 }
 
 long long aa_shell_cells(const AaArgs& a) {
