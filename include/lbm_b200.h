@@ -226,7 +226,10 @@ double lbm_b200_last_device_ms(KernelData *kd);
 long lbm_b200_last_launches(KernelData *kd);
 
 /* Bytes moved host->device and device->host by the last Kernel call (mirror
- * upload of a dirty mirror, download after the steps). */
+ * upload of a dirty mirror, download after the steps). List layouts move only
+ * the node range [0, nFluid) of each direction's plane of nCells elements
+ * (the padding behind the nodes holds no state): 19 * nFluid * element bytes
+ * each way; full-array layouts move the whole array. */
 void lbm_b200_last_copy_bytes(KernelData *kd, size_t *h2d, size_t *d2h);
 
 /* Lost device state. The kernels' bounded waits (bulk copies into shared

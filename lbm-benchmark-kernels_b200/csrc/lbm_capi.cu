@@ -363,7 +363,7 @@ long enqueue_steps(Gpu* g, const lbm::Trt<double>& t, int n, cudaEvent_t* ev = n
   };
   if (g->kind == kAa) {
     lbm::AaArgs a = aa_args(g);
-    const bool shell = lbm::aa_shell_cells(a) > 0;
+    const bool shell = lbm::aa_shell_needed(a);
     for (int it = 0; it < n; it += 2) {
       mark();
       lbm::aa_even_fp64(a, t, g->stream);
@@ -437,37 +437,65 @@ long launches_for(Gpu* g, int n) {
   long perPair = 2;
   if (g->kind == kAa) {
     const lbm::AaArgs a = aa_args(g);
-    perPair = 1 + (g->nOddItems > 0) + (lbm::aa_shell_cells(a) > 0 ? 1 : 0);
+    perPair = 1 + (g->nOddItems > 0) + (lbm::aa_shell_needed(a) ? 1 : 0);
   }
   return perPair * ((n + 1) / 2);
 }
 
+// Elements of each direction's plane that hold state. A list layout keeps its
+// nodes in [0, nFluid) of a plane of nCells elements; the padding behind them
+// is read by no step, so the field copies and conversions skip it (22 % of
+// the FP64 field of a 256^3 sphere packing at porosity 0.40). Full-array
+// layouts and list slabs (whose ghost slots follow the nodes) use whole
+// planes.
+size_t plane_elems(const Gpu* g) { return g->mirrorElems / Q; }
+size_t live_per_plane(const Gpu* g) {
+  return (!full_array(g->kind) && !g->listSlab) ? static_cast<size_t>(g->nFluid) : plane_elems(g);
+}
+
+// Copies the live part of the field between host and device on the
+// instance's stream (one 2D copy over the 19 planes, or one flat copy when
+// no padding is skipped); returns the bytes moved.
+size_t field_copy(Gpu* g, void* dst, const void* src, cudaMemcpyKind dir) {
+  const size_t plane = plane_elems(g), live = live_per_plane(g), eb = g->elemBytes;
+  if (live == plane || plane * eb > static_cast<size_t>(INT32_MAX)) {
+    LBM_CK(cudaMemcpyAsync(dst, src, g->mirrorElems * eb, dir, g->stream));
+    return g->mirrorElems * eb;
+  }
+  if (live > 0) LBM_CK(cudaMemcpy2DAsync(dst, plane * eb, src, plane * eb, live * eb, Q, dir, g->stream));
+  return Q * live * eb;
+}
+
 // Host-side conversion between the FP64 mirror and the device storage format
-// (element k belongs to direction k / nCells).
+// (element k of plane d belongs to direction d), over the live elements.
 void mirror_to_raw(Gpu* g) {
-  const size_t n = g->mirrorElems, nc = (size_t)g->nCells;
-  if (g->storage == lbm::kStoreF32) {
-    float* r = static_cast<float*>(g->rawStage);
-    for (size_t k = 0; k < n; ++k) r[k] = (float)(g->mirror[k] - weight_of((int)(k / nc)));
-  } else {
-    uint16_t* r = static_cast<uint16_t*>(g->rawStage);
-    for (size_t k = 0; k < n; ++k) {
-      const int d = (int)(k / nc);
-      r[k] = lbmh_f32_to_f16((float)((g->mirror[k] - weight_of(d)) * f16_scale_of(d)));
+  const size_t nc = plane_elems(g), live = live_per_plane(g);
+  for (int d = 0; d < Q; ++d) {
+    const double* m = g->mirror + d * nc;
+    const double w = weight_of(d);
+    if (g->storage == lbm::kStoreF32) {
+      float* r = static_cast<float*>(g->rawStage) + d * nc;
+      for (size_t k = 0; k < live; ++k) r[k] = (float)(m[k] - w);
+    } else {
+      uint16_t* r = static_cast<uint16_t*>(g->rawStage) + d * nc;
+      const double sc = f16_scale_of(d);
+      for (size_t k = 0; k < live; ++k) r[k] = lbmh_f32_to_f16((float)((m[k] - w) * sc));
     }
   }
 }
 
 void raw_to_mirror(Gpu* g) {
-  const size_t n = g->mirrorElems, nc = (size_t)g->nCells;
-  if (g->storage == lbm::kStoreF32) {
-    const float* r = static_cast<const float*>(g->rawStage);
-    for (size_t k = 0; k < n; ++k) g->mirror[k] = weight_of((int)(k / nc)) + (double)r[k];
-  } else {
-    const uint16_t* r = static_cast<const uint16_t*>(g->rawStage);
-    for (size_t k = 0; k < n; ++k) {
-      const int d = (int)(k / nc);
-      g->mirror[k] = weight_of(d) + (double)lbmh_f16_to_f32(r[k]) / f16_scale_of(d);
+  const size_t nc = plane_elems(g), live = live_per_plane(g);
+  for (int d = 0; d < Q; ++d) {
+    double* m = g->mirror + d * nc;
+    const double w = weight_of(d);
+    if (g->storage == lbm::kStoreF32) {
+      const float* r = static_cast<const float*>(g->rawStage) + d * nc;
+      for (size_t k = 0; k < live; ++k) m[k] = w + (double)r[k];
+    } else {
+      const uint16_t* r = static_cast<const uint16_t*>(g->rawStage) + d * nc;
+      const double sc = f16_scale_of(d);
+      for (size_t k = 0; k < live; ++k) m[k] = w + (double)lbmh_f16_to_f32(r[k]) / sc;
     }
   }
 }
@@ -489,18 +517,16 @@ void upload_if_dirty(Gpu* g) {
     mirror_to_raw(g);
     src = g->rawStage;
   }
-  LBM_CK(cudaMemcpyAsync(current_grid(g), src, g->mirrorElems * g->elemBytes, cudaMemcpyHostToDevice, g->stream));
-  g->lastH2D = g->mirrorElems * g->elemBytes;
+  g->lastH2D = field_copy(g, current_grid(g), src, cudaMemcpyHostToDevice);
   g->dirty = false;
   clear_lost(g);
 }
 
 void download(Gpu* g) {
   void* dst = g->storage == lbm::kStoreF64 ? static_cast<void*>(g->mirror) : g->rawStage;
-  LBM_CK(cudaMemcpyAsync(dst, current_grid(g), g->mirrorElems * g->elemBytes, cudaMemcpyDeviceToHost, g->stream));
+  g->lastD2H = field_copy(g, dst, current_grid(g), cudaMemcpyDeviceToHost);
   LBM_CK(cudaStreamSynchronize(g->stream));
   if (g->storage != lbm::kStoreF64) raw_to_mirror(g);
-  g->lastD2H = g->mirrorElems * g->elemBytes;
 }
 
 // Reads the device error word (synchronous); a non-zero word marks the
@@ -1323,7 +1349,7 @@ int lbm_aa_slab_step(KernelData* kd, CaseData* cd, int half, void* stream) {
     lbm::aa_even_fp64(a, t, s);
   } else {
     if (g->nOddItems > 0) lbm::aa_odd_interior_fp64(a, t, g->dOddItems, g->nOddItems, g->dOddCells, s);
-    if (lbm::aa_shell_cells(a) > 0) lbm::aa_odd_face_fp64(a, t, s);
+    if (lbm::aa_shell_needed(a)) lbm::aa_odd_face_fp64(a, t, s);
     g->iteration += 2;
   }
   return (int)cudaGetLastError();
@@ -1409,7 +1435,7 @@ int lbm_aa_slab_odd_part(KernelData* kd, CaseData* cd, int part, void* stream) {
     if (part == 0) {
       // the interior blocks read and write only the slab's own planes
       if (g->nOddItems > 0) lbm::aa_odd_interior_fp64(a, t, g->dOddItems, g->nOddItems, g->dOddCells, s);
-    } else if (lbm::aa_shell_cells(a) > 0) {
+    } else if (lbm::aa_shell_needed(a)) {
       lbm::aa_odd_face_fp64(a, t, s);
     }
   }

@@ -191,6 +191,9 @@ bool aa_has_interior(const AaArgs& a);
 void fa_push_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
 void fa_pull_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
 long long aa_shell_cells(const AaArgs& a);
+// Whether the face kernel has cells to take: some shell cell lies outside the
+// interior launch's range (the faces of non-periodic axes and halo faces).
+bool aa_shell_needed(const AaArgs& a);
 void list_even_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
 void list_odd_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
 void list_pull_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);

@@ -89,27 +89,35 @@ __global__ void __launch_bounds__(kAaEvenBlock, 1024 / kAaEvenBlock) k_aa_even_f
 // (x + c_i, i) with the increment of i, or -- bounced back at a wall -- to
 // its own slot (x, inv(i)) with the increment of inv(i).
 //
-// Two launches share the step. The interior launch takes every cell off the
-// x and y faces -- and off the z faces too unless z is periodic: links of
-// these cells leave the domain at most through a periodic z face, which is a
-// fixed offset of -/+ nZ cells. Interior cells are sorted on the host by
-// their link words: a cell without reversed links is "direct" (every address
-// is the neighbour's slot), the others are "general" (each address is a
-// select between the neighbour's slot and the node's own slot). The launch
-// runs a list of work items in x-plane order: for each plane, the blocks
-// (128 z-cells of one row) that hold at least one direct cell -- these skip
-// the general cells in them -- then chunks of 128 of the plane's general
-// cells, one thread per cell. So the select-free path covers every direct
-// cell, also those next to a wall (in a 256^3 channel a split by whole blocks
-// sends 27 % of the cells, every block with one wall-adjacent cell, down the
-// general path; the general cells are 1.6 %), and a general cell runs while
-// the direct blocks of its plane touch the same 32-byte sectors, so its
-// scattered accesses (a column of wall-adjacent cells is `pitch` apart) hit
-// L2 instead of DRAM. Blocks without fluid cells are not launched. In both
-// paths the 19 loads are issued together. The face kernel takes the
-// remaining shell: links that leave the domain wrap periodically on every
-// crossed axis, or, at a non-periodic face, go to the ghost layer (an "open"
-// link), as in the reference.
+// Two launches share the step. The interior launch takes every cell whose
+// links leave the domain, if at all, only through periodic faces
+// (aa_interior_range): the z faces when z is periodic, and the x and y faces
+// too when every axis is periodic and no x face is a halo face (then the
+// face launch has no cells left). A link through such a face moves by a
+// fixed -/+ n cells along each crossed axis. (Taking the periodic x faces of
+// a channel, periodic in x only, into the interior saves nothing: the face
+// launch still runs for its wall faces, and the interior pays for the wrap
+// tests of two more axes -- 256^3 channel odd step 0.873 + 0.029 ms against
+// 0.862 + 0.029 ms; on the fully periodic box the face launch goes away,
+// 0.813 + 0.039 -> 0.824 ms.) Interior cells are sorted on the
+// host by their link words: a cell without reversed links is "direct" (every
+// address is the neighbour's slot), the others are "general" (each address
+// is a select between the neighbour's slot and the node's own slot). The
+// launch runs a list of work items in x-plane order: for each plane, the
+// blocks (128 z-cells of one row) that hold at least one direct cell --
+// these skip the general cells in them -- then chunks of 128 of the plane's
+// general cells, one thread per cell. So the select-free path covers every
+// direct cell, also those next to a wall (in a 256^3 channel a split by
+// whole blocks sends 27 % of the cells, every block with one wall-adjacent
+// cell, down the general path; the general cells are 1.6 %), and a general
+// cell runs while the direct blocks of its plane touch the same 32-byte
+// sectors, so its scattered accesses (a column of wall-adjacent cells is
+// `pitch` apart) hit L2 instead of DRAM. Blocks without fluid cells are not
+// launched. In both paths the 19 loads are issued together. The face kernel
+// takes the remaining shell (skipping the cells the interior launch covers):
+// links that leave the domain wrap periodically on every crossed axis, or,
+// at a non-periodic face, go to the ghost layer (an "open" link), as in the
+// reference.
 //
 // Cells of different nodes never share a slot in the odd step (each node
 // reads and writes only its own links' slots), so the work items and the
@@ -120,33 +128,74 @@ __global__ void __launch_bounds__(kAaEvenBlock, 1024 / kAaEvenBlock) k_aa_even_f
 // 0.818 ms for 64 x 2 and 0.830 ms for 32 x 4 blocks (256^3 fluid box, B200).
 constexpr int kAaBZ = 128, kAaBY = 1;
 
-// Interior block `id` of the list: (bz, by, bx) with bz fastest.
-__device__ __forceinline__ void aa_interior_block(const AaArgs& a, int id, int& z, int& y, int& x) {
-  const int nz = a.perZ ? a.nZ : a.nZ - 2;
-  const int gz = (nz + kAaBZ - 1) / kAaBZ, gy = (a.nY - 2 + kAaBY - 1) / kAaBY;
-  const int bz = id % gz, rest = id / gz;
-  z = (a.perZ ? 0 : 1) + bz * kAaBZ + threadIdx.x;
-  y = 1 + (rest % gy) * kAaBY + threadIdx.y;
-  x = 1 + rest / gy;
+// Whether the interior launch takes the whole lattice (see above).
+__host__ __device__ __forceinline__ bool aa_interior_all(const AaArgs& a) {
+  return a.perX && a.perY && a.perZ && !a.haloLo && !a.haloHi;
 }
 
-// The periodic z wrap of an interior cell, decided once per cell: a link
-// with c_z = -1 leaving through z = 0 moves +nZ cells, one with c_z = +1
-// through z = nZ-1 moves -nZ (only reachable when z is periodic: otherwise
-// interior cells are off the z faces).
-struct ZWrap {
-  int down, up;
-  __device__ __forceinline__ ZWrap(const AaArgs& a, int z)
-      : down(z == 0 ? a.nZ : 0), up(z == a.nZ - 1 ? -a.nZ : 0) {}
-  __device__ __forceinline__ int operator()(int d) const { return cz(d) < 0 ? down : (cz(d) > 0 ? up : 0); }
+// The interior ranges [lo, hi] of x, y and z (see above).
+struct AaRange {
+  int x0, x1, y0, y1, z0, z1;
+};
+__host__ __device__ __forceinline__ AaRange aa_interior_range(const AaArgs& a) {
+  AaRange r;
+  const bool all = aa_interior_all(a);
+  r.x0 = all ? 0 : 1;
+  r.x1 = all ? a.nX - 1 : a.nX - 2;
+  r.y0 = all ? 0 : 1;
+  r.y1 = all ? a.nY - 1 : a.nY - 2;
+  r.z0 = a.perZ ? 0 : 1;
+  r.z1 = a.perZ ? a.nZ - 1 : a.nZ - 2;
+  return r;
+}
+
+// Interior block `id` of the list: (bz, by, bx) with bz fastest.
+__device__ __forceinline__ void aa_interior_block(const AaArgs& a, const AaRange& r, int id, int& z, int& y,
+                                                  int& x) {
+  const int gz = (r.z1 - r.z0 + 1 + kAaBZ - 1) / kAaBZ, gy = (r.y1 - r.y0 + 1 + kAaBY - 1) / kAaBY;
+  const int bz = id % gz, rest = id / gz;
+  z = r.z0 + bz * kAaBZ + threadIdx.x;
+  y = r.y0 + (rest % gy) * kAaBY + threadIdx.y;
+  x = r.x0 + rest / gy;
+}
+
+// The periodic wraps of an interior cell, decided once per cell: a link with
+// c_a = -1 leaving through the low face of axis a moves +n_a cells along a,
+// one with c_a = +1 through the high face moves -n_a. kXY: the interior
+// includes the x and y faces (every axis periodic); otherwise only z faces
+// are reached.
+template <bool kXY>
+struct Wrap3 {
+  const AaArgs& a;
+  unsigned m;  // bits 0-5: x == 0, x == nX - 1, y == 0, y == nY - 1, z == 0, z == nZ - 1
+  __device__ __forceinline__ Wrap3(const AaArgs& a_, int x, int y, int z)
+      : a(a_),
+        m((kXY ? (x == 0) | (x == a_.nX - 1) << 1 | (y == 0) << 2 | (y == a_.nY - 1) << 3 : 0) | (z == 0) << 4 |
+          (z == a_.nZ - 1) << 5) {}
+  __device__ __forceinline__ int operator()(int d) const {
+    int o = 0;
+    if (kXY) {
+      if (cx(d) < 0 && (m & 1u)) o += a.nX * a.xs;
+      if (cx(d) > 0 && (m & 2u)) o -= a.nX * a.xs;
+      if (cy(d) < 0 && (m & 4u)) o += a.nY * a.pitch;
+      if (cy(d) > 0 && (m & 8u)) o -= a.nY * a.pitch;
+    }
+    if (cz(d) < 0 && (m & 16u)) o += a.nZ;
+    if (cz(d) > 0 && (m & 32u)) o -= a.nZ;
+    return o;
+  }
 };
 
 // A general cell (interior, fluid, at least one reversed link).
+template <bool kXY>
 __device__ __noinline__ void aa_odd_general_cell(const AaArgs& a, const Trt<double>& t, int c) {
-  const int z = c % a.pitch - kZOff;  // a row is `pitch` cells; interior z = 0 sits at kZOff
+  // cell index -> (x, y, z): planes of xs cells, rows of pitch cells, interior
+  // z = 0 at element kZOff
+  const int x = c / a.xs - 1, rem = c % a.xs;
+  const int y = rem / a.pitch - 1, z = rem % a.pitch - kZOff;
   const uint32_t w = __ldg(a.link + c);
   double* const fb = a.f + c;
-  const ZWrap wrap(a, z);
+  const Wrap3<kXY> wrap(a, x, y, z);
   const int S = (int)a.dstride;
   auto load = [&](int d) -> double {
     if (d == DC) return fb[a.ldOff[DC]] + t.force[DC];
@@ -169,31 +218,32 @@ __device__ __noinline__ void aa_odd_general_cell(const AaArgs& a, const Trt<doub
 
 // Work item `items[blockIdx.x]`: >= 0 a block id (direct cells), < 0 the
 // general-cell chunk ~item (cells[128 * chunk + thread], -1 = none).
-// Launch bounds: 7 resident blocks of 128 threads per SM (the direct path
-// takes 68 registers, no spills; measured fastest among 1-8 on B200; the
-// general path spills a few values into L1 under that cap). Direct addresses
-// are the cell's base pointer plus a per-direction offset from the parameter
-// bank (and the z wrap), so no per-direction address stays live in
-// registers; store addresses come from a laundered base pointer, apart from
-// the load addresses, so those need not stay live across the collision.
+// Launch bounds: 7 resident blocks of 128 threads per SM (measured fastest
+// among 1-8 on B200; the general path spills a few values into L1 under that
+// cap). Direct addresses are the cell's base pointer plus a per-direction
+// offset from the parameter bank (and the periodic wraps), so no
+// per-direction address stays live in registers; store addresses come from a
+// laundered base pointer, apart from the load addresses, so those need not
+// stay live across the collision.
+template <bool kXY>
 __global__ void __launch_bounds__(128, 7)
     k_aa_odd_interior_fp64(const __grid_constant__ AaArgs a, const __grid_constant__ Trt<double> t, const int* items,
                            const int* cells) {
   const int item = __ldg(items + blockIdx.x);
   if (item < 0) {
     const int c = __ldg(cells + (size_t)(~item) * 128 + threadIdx.y * kAaBZ + threadIdx.x);
-    if (c >= 0) aa_odd_general_cell(a, t, c);
+    if (c >= 0) aa_odd_general_cell<kXY>(a, t, c);
     return;
   }
+  const AaRange r = aa_interior_range(a);
   int x, y, z;
-  aa_interior_block(a, item, z, y, x);
-  const int zHi = a.perZ ? a.nZ - 1 : a.nZ - 2;
-  if (z > zHi || y > a.nY - 2) return;
+  aa_interior_block(a, r, item, z, y, x);
+  if (z > r.z1 || y > r.y1) return;
   const int c = aa_cell(a, x, y, z);
   const uint32_t w = __ldg(a.link + c);
   if ((w & (kFluidBit | kLinkBits)) != kFluidBit) return;  // solid, or a general cell (own item)
   double* const fb = a.f + c;
-  const ZWrap wrap(a, z);
+  const Wrap3<kXY> wrap(a, x, y, z);
   trt_update(t, [&](int d) -> double { return fb[a.ldOff[d] + wrap(inv(d))] + t.force[d]; },
              [&](int d, double v) { launder(fb)[a.stOff[d] + wrap(d)] = v + t.force[d]; });
 }
@@ -234,6 +284,8 @@ __global__ void __launch_bounds__(128) k_aa_odd_face_fp64(const AaArgs a, const 
   if (i >= nShell) return;
   int x, y, z;
   aa_shell_cell(a, i, x, y, z);
+  const AaRange r = aa_interior_range(a);
+  if (x >= r.x0 && x <= r.x1 && y >= r.y0 && y <= r.y1 && z >= r.z0 && z <= r.z1) return;  // the interior launch's
   const int c = aa_cell(a, x, y, z);
   const uint32_t w = __ldg(a.link + c);
   if (!(w & kFluidBit)) return;
@@ -448,12 +500,24 @@ long long aa_shell_cells(const AaArgs& a) {
   return sx * a.nY * a.nZ + sy * mx * a.nZ + (a.perZ ? 0 : sz * mx * my);
 }
 
-bool aa_has_interior(const AaArgs& a) { return a.nX > 2 && a.nY > 2 && (a.perZ || a.nZ > 2); }
+bool aa_has_interior(const AaArgs& a) {
+  const AaRange r = aa_interior_range(a);
+  return r.x1 >= r.x0 && r.y1 >= r.y0 && r.z1 >= r.z0;
+}
 
 long long aa_interior_block_count(const AaArgs& a) {
   if (!aa_has_interior(a)) return 0;
-  const long long nz = a.perZ ? a.nZ : a.nZ - 2;
-  return (nz + kAaBZ - 1) / kAaBZ * ((a.nY - 2 + kAaBY - 1) / kAaBY) * (long long)(a.nX - 2);
+  const AaRange r = aa_interior_range(a);
+  return (long long)((r.z1 - r.z0 + 1 + kAaBZ - 1) / kAaBZ) * ((r.y1 - r.y0 + 1 + kAaBY - 1) / kAaBY) *
+         (r.x1 - r.x0 + 1);
+}
+
+// Whether some shell cell lies outside the interior range (the face kernel
+// has work).
+bool aa_shell_needed(const AaArgs& a) {
+  if (aa_shell_cells(a) == 0) return false;
+  const AaRange r = aa_interior_range(a);
+  return r.x0 > 0 || r.x1 < a.nX - 1 || r.y0 > 0 || r.y1 < a.nY - 1 || r.z0 > 0 || r.z1 < a.nZ - 1;
 }
 
 void aa_interior_items(const AaArgs& a, const uint32_t* link, std::vector<int>& items, std::vector<int>& cells) {
@@ -461,30 +525,30 @@ void aa_interior_items(const AaArgs& a, const uint32_t* link, std::vector<int>& 
   cells.clear();
   const long long n = aa_interior_block_count(a);
   if (n == 0) return;
-  const int zLo = a.perZ ? 0 : 1, zHi = a.perZ ? a.nZ - 1 : a.nZ - 2;
-  const int gz = (zHi - zLo + 1 + kAaBZ - 1) / kAaBZ, gy = (a.nY - 2 + kAaBY - 1) / kAaBY;
+  const AaRange r = aa_interior_range(a);
+  const int gz = (r.z1 - r.z0 + 1 + kAaBZ - 1) / kAaBZ, gy = (r.y1 - r.y0 + 1 + kAaBY - 1) / kAaBY;
   const long long perPlane = (long long)gz * gy;
   auto word = [&](int x, int y, int z) { return link[(long long)(x + 1) * a.xs + (long long)(y + 1) * a.pitch + z + kZOff]; };
-  for (int x = 1; x <= a.nX - 2; ++x) {
+  for (int x = r.x0; x <= r.x1; ++x) {
     // the plane's blocks holding direct cells (block ids: bz fastest, then by, then x)
     for (long long k = 0; k < perPlane; ++k) {
       const int bz = (int)(k % gz), by = (int)(k / gz);
       bool direct = false;
       for (int ty = 0; ty < kAaBY && !direct; ++ty) {
-        const int y = 1 + by * kAaBY + ty;
-        if (y > a.nY - 2) break;
+        const int y = r.y0 + by * kAaBY + ty;
+        if (y > r.y1) break;
         for (int tz = 0; tz < kAaBZ; ++tz) {
-          const int z = zLo + bz * kAaBZ + tz;
-          if (z > zHi) break;
+          const int z = r.z0 + bz * kAaBZ + tz;
+          if (z > r.z1) break;
           if ((word(x, y, z) & (kFluidBit | kLinkBits)) == kFluidBit) { direct = true; break; }
         }
       }
-      if (direct) items.push_back((int)((x - 1) * perPlane + k));
+      if (direct) items.push_back((int)((x - r.x0) * perPlane + k));
     }
     // then the plane's general cells in chunks of 128
     const size_t first = cells.size();
-    for (int y = 1; y <= a.nY - 2; ++y)
-      for (int z = zLo; z <= zHi; ++z) {
+    for (int y = r.y0; y <= r.y1; ++y)
+      for (int z = r.z0; z <= r.z1; ++z) {
         const uint32_t w = word(x, y, z);
         if ((w & kFluidBit) && (w & kLinkBits)) cells.push_back((x + 1) * a.xs + (y + 1) * a.pitch + z + kZOff);
       }
@@ -508,7 +572,11 @@ void aa_even_fp64_planes(const AaArgs& a, const Trt<double>& t, int x0, int x1, 
 
 void aa_odd_interior_fp64(const AaArgs& a, const Trt<double>& t, const int* items, int nItems, const int* cells,
                           cudaStream_t s) {
-  if (nItems > 0) k_aa_odd_interior_fp64<<<nItems, dim3(kAaBZ, kAaBY), 0, s>>>(a, t, items, cells);
+  if (nItems <= 0) return;
+  if (aa_interior_all(a))
+    k_aa_odd_interior_fp64<true><<<nItems, dim3(kAaBZ, kAaBY), 0, s>>>(a, t, items, cells);
+  else
+    k_aa_odd_interior_fp64<false><<<nItems, dim3(kAaBZ, kAaBY), 0, s>>>(a, t, items, cells);
 }
 
 void aa_odd_face_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s) {
