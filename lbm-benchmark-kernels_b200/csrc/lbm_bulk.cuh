@@ -58,17 +58,19 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 }
 
 // Stages the run record of tile blockIdx.x + a.tileBase (run-compressed adjacency, see
-// kRunHdrWords) into srun (kRunTileWords words) with one bulk copy. A record
-// whose size does not fit flags error bit 4 and is not copied. After the
+// kRunHdrWords) into srun (kRunTileWords words) with one bulk copy, in two
+// halves: stage_run_tile_issue starts the copy (thread 0; a record whose size
+// does not fit flags error bit 4 and is not copied) and makes the barrier
+// visible to the block; stage_run_tile_wait waits for it. Work that does not
+// need the record (a node's own PDFs) may run between the two. After the
 // wait, warp 1 prefetches into L2 the record of the tile kWaves x
 // `a.prefetch` tiles ahead (kWaves = 1: the block that will take this one's
-// place), off the block's critical path. Returns false (error word set) if
-// the copy did not arrive within the spin limit or was refused; every thread
-// returns the same.
-template <int kWaves = 1, class A>
-__device__ __forceinline__ bool stage_run_tile(const A& a, uint32_t* srun, uint64_t* bar, int* ok) {
+// place), off the block's critical path. Both return false (error word set)
+// if the copy was refused or did not arrive within the spin limit; every
+// thread returns the same from the issue half.
+template <class A>
+__device__ __forceinline__ bool stage_run_tile_issue(const A& a, uint32_t* srun, uint64_t* bar, int* ok) {
   const unsigned tile = blockIdx.x + static_cast<unsigned>(a.tileBase);
-  const unsigned nTiles = static_cast<unsigned>((a.nFluid + kListTile - 1) / kListTile);
   if (threadIdx.x == 0) {
     const uint32_t o0 = a.runOff[tile], o1 = a.runOff[tile + 1];
     const uint32_t bytes = (o1 - o0) * 16u;
@@ -82,11 +84,17 @@ __device__ __forceinline__ bool stage_run_tile(const A& a, uint32_t* srun, uint6
     }
   }
   __syncthreads();
-  if (!*ok) return false;
+  return *ok != 0;
+}
+
+template <int kWaves = 1, class A>
+__device__ __forceinline__ bool stage_run_tile_wait(const A& a, uint64_t* bar) {
   if (!mbar_wait_bounded(bar, 0)) {
-    if (threadIdx.x == 0) atomicOr(a.err, 1);
+    atomicOr(a.err, 1);
     return false;
   }
+  const unsigned tile = blockIdx.x + static_cast<unsigned>(a.tileBase);
+  const unsigned nTiles = static_cast<unsigned>((a.nFluid + kListTile - 1) / kListTile);
   if (threadIdx.x == 32 && a.prefetch > 0 && tile + kWaves * static_cast<unsigned>(a.prefetch) < nTiles) {
     const unsigned t = tile + kWaves * a.prefetch;
     const uint32_t o0 = a.runOff[t], o1 = a.runOff[t + 1];
@@ -94,6 +102,13 @@ __device__ __forceinline__ bool stage_run_tile(const A& a, uint32_t* srun, uint6
       bulk_prefetch_l2(a.runs + static_cast<size_t>(o0) * 4, (o1 - o0) * 16u);
   }
   return true;
+}
+
+// Both halves back to back (the record is needed from the start).
+template <int kWaves = 1, class A>
+__device__ __forceinline__ bool stage_run_tile(const A& a, uint32_t* srun, uint64_t* bar, int* ok) {
+  if (!stage_run_tile_issue(a, srun, bar, ok)) return false;
+  return stage_run_tile_wait<kWaves>(a, bar);
 }
 
 // The adjacency row of node `tid` of a staged run record and the node's

@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(kAaEvenBlock, 1024 / kAaEvenBlock) k_aa_even_f
 // sectors, so its scattered accesses (a column of wall-adjacent cells is
 // `pitch` apart) hit L2 instead of DRAM. Blocks without fluid cells are not
 // launched. In both paths the 19 loads are issued together. The face kernel
-// takes the remaining shell (skipping the cells the interior launch covers):
+// takes the shell (x and y faces, and z faces unless z is periodic):
 // links that leave the domain wrap periodically on every crossed axis, or,
 // at a non-periodic face, go to the ghost layer (an "open" link), as in the
 // reference.
@@ -161,41 +161,58 @@ __device__ __forceinline__ void aa_interior_block(const AaArgs& a, const AaRange
 
 // The periodic wraps of an interior cell, decided once per cell: a link with
 // c_a = -1 leaving through the low face of axis a moves +n_a cells along a,
-// one with c_a = +1 through the high face moves -n_a. kXY: the interior
-// includes the x and y faces (every axis periodic); otherwise only z faces
-// are reached.
-template <bool kXY>
-struct Wrap3 {
+// one with c_a = +1 through the high face moves -n_a. ZWrap: only z faces
+// are reached (interior cells are off the x and y faces, and off the z faces
+// unless z is periodic); XyzWrap: the interior is the whole lattice.
+struct ZWrap {
+  int down, up;
+  __device__ __forceinline__ ZWrap(const AaArgs& a, int z)
+      : down(z == 0 ? a.nZ : 0), up(z == a.nZ - 1 ? -a.nZ : 0) {}
+  __device__ __forceinline__ int operator()(int d) const { return cz(d) < 0 ? down : (cz(d) > 0 ? up : 0); }
+};
+struct XyzWrap {
   const AaArgs& a;
   unsigned m;  // bits 0-5: x == 0, x == nX - 1, y == 0, y == nY - 1, z == 0, z == nZ - 1
-  __device__ __forceinline__ Wrap3(const AaArgs& a_, int x, int y, int z)
+  __device__ __forceinline__ XyzWrap(const AaArgs& a_, int x, int y, int z)
       : a(a_),
-        m((kXY ? (x == 0) | (x == a_.nX - 1) << 1 | (y == 0) << 2 | (y == a_.nY - 1) << 3 : 0) | (z == 0) << 4 |
+        m((x == 0) | (x == a_.nX - 1) << 1 | (y == 0) << 2 | (y == a_.nY - 1) << 3 | (z == 0) << 4 |
           (z == a_.nZ - 1) << 5) {}
   __device__ __forceinline__ int operator()(int d) const {
     int o = 0;
-    if (kXY) {
-      if (cx(d) < 0 && (m & 1u)) o += a.nX * a.xs;
-      if (cx(d) > 0 && (m & 2u)) o -= a.nX * a.xs;
-      if (cy(d) < 0 && (m & 4u)) o += a.nY * a.pitch;
-      if (cy(d) > 0 && (m & 8u)) o -= a.nY * a.pitch;
-    }
+    if (cx(d) < 0 && (m & 1u)) o += a.nX * a.xs;
+    if (cx(d) > 0 && (m & 2u)) o -= a.nX * a.xs;
+    if (cy(d) < 0 && (m & 4u)) o += a.nY * a.pitch;
+    if (cy(d) > 0 && (m & 8u)) o -= a.nY * a.pitch;
     if (cz(d) < 0 && (m & 16u)) o += a.nZ;
     if (cz(d) > 0 && (m & 32u)) o -= a.nZ;
     return o;
   }
 };
+template <bool kXY>
+__device__ __forceinline__ auto aa_wrap(const AaArgs& a, int x, int y, int z) {
+  if constexpr (kXY)
+    return XyzWrap(a, x, y, z);
+  else
+    return ZWrap(a, z);
+}
 
 // A general cell (interior, fluid, at least one reversed link).
 template <bool kXY>
 __device__ __noinline__ void aa_odd_general_cell(const AaArgs& a, const Trt<double>& t, int c) {
-  // cell index -> (x, y, z): planes of xs cells, rows of pitch cells, interior
-  // z = 0 at element kZOff
-  const int x = c / a.xs - 1, rem = c % a.xs;
-  const int y = rem / a.pitch - 1, z = rem % a.pitch - kZOff;
+  // cell index -> (x, y, z): planes of xs cells, rows of pitch cells,
+  // interior z = 0 at element kZOff (x and y only matter to XyzWrap)
+  int x = 0, y = 0, z;
+  if constexpr (kXY) {
+    const int rem = c % a.xs;
+    x = c / a.xs - 1;
+    y = rem / a.pitch - 1;
+    z = rem % a.pitch - kZOff;
+  } else {
+    z = c % a.pitch - kZOff;
+  }
   const uint32_t w = __ldg(a.link + c);
   double* const fb = a.f + c;
-  const Wrap3<kXY> wrap(a, x, y, z);
+  const auto wrap = aa_wrap<kXY>(a, x, y, z);
   const int S = (int)a.dstride;
   auto load = [&](int d) -> double {
     if (d == DC) return fb[a.ldOff[DC]] + t.force[DC];
@@ -243,7 +260,7 @@ __global__ void __launch_bounds__(128, 7)
   const uint32_t w = __ldg(a.link + c);
   if ((w & (kFluidBit | kLinkBits)) != kFluidBit) return;  // solid, or a general cell (own item)
   double* const fb = a.f + c;
-  const Wrap3<kXY> wrap(a, x, y, z);
+  const auto wrap = aa_wrap<kXY>(a, x, y, z);
   trt_update(t, [&](int d) -> double { return fb[a.ldOff[d] + wrap(inv(d))] + t.force[d]; },
              [&](int d, double v) { launder(fb)[a.stOff[d] + wrap(d)] = v + t.force[d]; });
 }
@@ -284,8 +301,6 @@ __global__ void __launch_bounds__(128) k_aa_odd_face_fp64(const AaArgs a, const 
   if (i >= nShell) return;
   int x, y, z;
   aa_shell_cell(a, i, x, y, z);
-  const AaRange r = aa_interior_range(a);
-  if (x >= r.x0 && x <= r.x1 && y >= r.y0 && y <= r.y1 && z >= r.z0 && z <= r.z1) return;  // the interior launch's
   const int c = aa_cell(a, x, y, z);
   const uint32_t w = __ldg(a.link + c);
   if (!(w & kFluidBit)) return;
@@ -512,13 +527,10 @@ long long aa_interior_block_count(const AaArgs& a) {
          (r.x1 - r.x0 + 1);
 }
 
-// Whether some shell cell lies outside the interior range (the face kernel
-// has work).
-bool aa_shell_needed(const AaArgs& a) {
-  if (aa_shell_cells(a) == 0) return false;
-  const AaRange r = aa_interior_range(a);
-  return r.x0 > 0 || r.x1 < a.nX - 1 || r.y0 > 0 || r.y1 < a.nY - 1 || r.z0 > 0 || r.z1 < a.nZ - 1;
-}
+// Whether the face kernel has work: the shell (x and y faces, z faces unless
+// z is periodic) lies outside the interior range unless the interior is the
+// whole lattice.
+bool aa_shell_needed(const AaArgs& a) { return !aa_interior_all(a) && aa_shell_cells(a) > 0; }
 
 void aa_interior_items(const AaArgs& a, const uint32_t* link, std::vector<int>& items, std::vector<int>& cells) {
   items.clear();
@@ -683,19 +695,26 @@ __global__ void __launch_bounds__(kListTile) k_list_pull_fp64(const ListArgs a, 
 // the node's own 19 PDFs from the source grid, each post-collision PDF
 // written through the push adjacency into the destination grid with the
 // body-force increment of the slot's direction (a bounce back lands in the
-// node's own slot inv(d) and gets the increment of inv(d)).
+// node's own slot inv(d) and gets the increment of inv(d)). The own PDFs do
+// not depend on the adjacency: their loads are issued before the wait for
+// the tile's run record, so the two latencies overlap.
 __global__ void __launch_bounds__(kListTile, 3) k_list_push_fp64(const ListArgs a, const Trt<double> t) {
   __shared__ alignas(128) uint32_t srun[kRunTileWords];
   __shared__ alignas(8) uint64_t bar;
   __shared__ int ok;
-  if (!stage_run_tile(a, srun, &bar, &ok)) return;
+  if (!stage_run_tile_issue(a, srun, &bar, &ok)) return;
   const int n = (blockIdx.x + a.tileBase) * kListTile + threadIdx.x;
-  if (n >= a.nFluid) return;
+  const long long S = a.nCells;
+  double x[Q];
+  if (n < a.nFluid) {
+    const double* const f = a.f + n;
+#pragma unroll
+    for (int d = 0; d < Q; ++d) x[d] = f[d * S];
+  }
+  if (!stage_run_tile_wait(a, &bar) || n >= a.nFluid) return;
   uint32_t off;
   const uint32_t* e = run_row(srun, threadIdx.x, off);
-  const double* const f = a.f + n;
   double* const g = a.g;
-  const long long S = a.nCells;
   auto store = [&](int d, double v) {
     if (d == DC) { g[DC * S + n] = v + t.force[DC]; return; }
     const uint32_t dst = reinterpret_cast<const volatile uint32_t*>(e)[d] + off;
@@ -703,7 +722,7 @@ __global__ void __launch_bounds__(kListTile, 3) k_list_push_fp64(const ListArgs 
     const bool bounce = dst == static_cast<uint32_t>(j * S + n);
     g[dst] = v + (bounce ? t.force[j] : t.force[d]);
   };
-  trt_update(t, [&](int d) { return f[d * S]; }, store);
+  trt_update(t, [&](int d) { return x[d]; }, store);
 }
 
 template <typename E>
