@@ -28,7 +28,7 @@ __device__ __forceinline__ void tile_store(BatchTile* dst, uint32_t w) {
 
 template <class St>
 __device__ __forceinline__ void batch_even_node(const BatchTile& T, int n) {
-  lp_even_node<St>(static_cast<typename St::T*>(T.f), T.nCells, n, TrtDev<St>(T.trt));
+  lp_even_node<St, false>(static_cast<typename St::T*>(T.f), T.nCells, n, TrtDev<St>(T.trt));
 }
 
 // Grid-stride over the tiles; with one block per tile the loop runs once.
@@ -67,7 +67,7 @@ template <class St>
 __device__ __forceinline__ void batch_odd_node(const BatchTile& T, const uint32_t* srun, int local) {
   uint32_t off;
   const uint32_t* e = run_row(srun, local, off);
-  lp_odd_node<St>(static_cast<typename St::T*>(T.f), static_cast<uint32_t>(T.nCells), T.n0 + local, e, off,
+  lp_odd_node<St, false>(static_cast<typename St::T*>(T.f), static_cast<uint32_t>(T.nCells), T.n0 + local, e, off,
                   TrtDev<St>(T.trt));
 }
 

