@@ -191,8 +191,9 @@ bool aa_has_interior(const AaArgs& a);
 void fa_push_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
 void fa_pull_fp64(const AaArgs& a, const Trt<double>& t, cudaStream_t s);
 long long aa_shell_cells(const AaArgs& a);
-// Whether the face kernel has cells to take: some shell cell lies outside the
-// interior launch's range (the faces of non-periodic axes and halo faces).
+// Whether the face kernel has cells to take: the shell exists and the
+// interior launch does not cover the whole lattice (it does when every axis
+// is periodic and no x face is a halo face).
 bool aa_shell_needed(const AaArgs& a);
 void list_even_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
 void list_odd_fp64(const ListArgs& a, const Trt<double>& t, cudaStream_t s);
