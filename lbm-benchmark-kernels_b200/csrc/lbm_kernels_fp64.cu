@@ -149,12 +149,18 @@ __host__ __device__ __forceinline__ AaRange aa_interior_range(const AaArgs& a) {
   return r;
 }
 
+// Interior blocks start at z = 0 whatever the interior's first z: row
+// element kZOff + z then puts each warp's 32 cells on whole 32-byte sectors
+// (with walls in z, a start at z = 1 made every warp's z-aligned accesses
+// span one sector more); threads off the interior range return.
+__host__ __device__ __forceinline__ int aa_interior_zblocks(const AaArgs& a) { return (a.nZ + kAaBZ - 1) / kAaBZ; }
+
 // Interior block `id` of the list: (bz, by, bx) with bz fastest.
 __device__ __forceinline__ void aa_interior_block(const AaArgs& a, const AaRange& r, int id, int& z, int& y,
                                                   int& x) {
-  const int gz = (r.z1 - r.z0 + 1 + kAaBZ - 1) / kAaBZ, gy = (r.y1 - r.y0 + 1 + kAaBY - 1) / kAaBY;
+  const int gz = aa_interior_zblocks(a), gy = (r.y1 - r.y0 + 1 + kAaBY - 1) / kAaBY;
   const int bz = id % gz, rest = id / gz;
-  z = r.z0 + bz * kAaBZ + threadIdx.x;
+  z = bz * kAaBZ + threadIdx.x;
   y = r.y0 + (rest % gy) * kAaBY + threadIdx.y;
   x = r.x0 + rest / gy;
 }
@@ -255,7 +261,7 @@ __global__ void __launch_bounds__(128, 7)
   const AaRange r = aa_interior_range(a);
   int x, y, z;
   aa_interior_block(a, r, item, z, y, x);
-  if (z > r.z1 || y > r.y1) return;
+  if (z < r.z0 || z > r.z1 || y > r.y1) return;
   const int c = aa_cell(a, x, y, z);
   const uint32_t w = __ldg(a.link + c);
   if ((w & (kFluidBit | kLinkBits)) != kFluidBit) return;  // solid, or a general cell (own item)
@@ -523,8 +529,7 @@ bool aa_has_interior(const AaArgs& a) {
 long long aa_interior_block_count(const AaArgs& a) {
   if (!aa_has_interior(a)) return 0;
   const AaRange r = aa_interior_range(a);
-  return (long long)((r.z1 - r.z0 + 1 + kAaBZ - 1) / kAaBZ) * ((r.y1 - r.y0 + 1 + kAaBY - 1) / kAaBY) *
-         (r.x1 - r.x0 + 1);
+  return (long long)aa_interior_zblocks(a) * ((r.y1 - r.y0 + 1 + kAaBY - 1) / kAaBY) * (r.x1 - r.x0 + 1);
 }
 
 // Whether the face kernel has work: the shell (x and y faces, z faces unless
@@ -538,7 +543,7 @@ void aa_interior_items(const AaArgs& a, const uint32_t* link, std::vector<int>& 
   const long long n = aa_interior_block_count(a);
   if (n == 0) return;
   const AaRange r = aa_interior_range(a);
-  const int gz = (r.z1 - r.z0 + 1 + kAaBZ - 1) / kAaBZ, gy = (r.y1 - r.y0 + 1 + kAaBY - 1) / kAaBY;
+  const int gz = aa_interior_zblocks(a), gy = (r.y1 - r.y0 + 1 + kAaBY - 1) / kAaBY;
   const long long perPlane = (long long)gz * gy;
   auto word = [&](int x, int y, int z) { return link[(long long)(x + 1) * a.xs + (long long)(y + 1) * a.pitch + z + kZOff]; };
   for (int x = r.x0; x <= r.x1; ++x) {
@@ -550,7 +555,8 @@ void aa_interior_items(const AaArgs& a, const uint32_t* link, std::vector<int>& 
         const int y = r.y0 + by * kAaBY + ty;
         if (y > r.y1) break;
         for (int tz = 0; tz < kAaBZ; ++tz) {
-          const int z = r.z0 + bz * kAaBZ + tz;
+          const int z = bz * kAaBZ + tz;
+          if (z < r.z0) continue;
           if (z > r.z1) break;
           if ((word(x, y, z) & (kFluidBit | kLinkBits)) == kFluidBit) { direct = true; break; }
         }
